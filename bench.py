@@ -1,0 +1,367 @@
+"""Benchmark: L-BFGS relaxations per second at n = 200.
+
+Workload (one "step"): relax a population of E = 4096 packings of n = 200
+trees (seeded uniform poses in a square of side 1.3 sqrt(n * tree area),
+theta uniform in [0, 360) deg), history m = 10, 200 iterations, fixed square
+side, cost = boundary distance + overlap area (+ 1e-2 h0^2, inactive with a
+fixed side) -- OptimizerBFGS's default objective (pack_dynamics.py:45-51).
+Synthetic data: the reference publishes no dataset.
+
+ours (default): the fused one-launch relaxation (packing_b200.relax).  Also
+  reported: e2e through the public API from pinned host buffers, the plain
+  drop-in (reference-style lbfgs loop over the same cost kernel), the FP32
+  roofline of the relaxation kernel, the CPU oracle baseline.
+--impl reference: the reference's CPU implementation of the path, i.e. the
+  FP64 C restatement of its cost kernels driven by the restatement of its
+  lbfgs, on the host cores (the reference has no other CPU path that runs
+  here: its own CPU cost needs shapely, which is absent).
+
+Multi-GPU (torchrun): every rank relaxes its own E packings (weak scaling,
+no data-path collective); value = all ranks' relaxations / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TREE_AREA = 0.2456875
+METRIC = "L-BFGS relaxations/sec at n=200 (batched vs plain, same GPU); p50/p99 serve latency"
+
+
+def workload(E, n, seed):
+    rng = np.random.default_rng(seed)
+    s = 1.3 * np.sqrt(n * TREE_AREA)
+    xy = rng.uniform(-s / 2, s / 2, size=(E, n, 2))
+    th = np.deg2rad(rng.uniform(0.0, 360.0, size=(E, n, 1)))
+    xyt = np.concatenate([xy, th], 2).astype(np.float32)
+    h = np.zeros((E, 3), np.float32)
+    h[:, 0] = np.sqrt((0.317 + 0.206 / np.sqrt(n)) * n * np.sqrt(1.1))
+    return xyt, h
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp32_peak_tflops(torch, L, dev):
+    """Measured FP32 FMA throughput of this GPU (TFLOP/s), best of 5."""
+    import ctypes
+    props = torch.cuda.get_device_properties(dev)
+    blocks, threads, iters = props.multi_processor_count * 8, 256, 20000
+    out = torch.empty(blocks, device=dev)
+    st = torch.cuda.current_stream(dev)
+    best = 0.0
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        rc = L.pk_fma_probe(ctypes.c_void_p(out.data_ptr()), blocks, threads, iters,
+                            ctypes.c_void_p(st.cuda_stream))
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        assert rc == 0
+        ms = e0.elapsed_time(e1)
+        best = max(best, blocks * threads * iters * 16 / (ms * 1e-3) / 1e12)
+    return best
+
+
+def cpu_baseline_relax(E, n, iters, history, seed=123):
+    """The FP64 oracle relaxing a bounded sample of the same workload."""
+    from oracle import oracle as O
+    xyt, h = workload(E, n, seed)
+    x0 = np.concatenate([xyt.reshape(E, -1), h], 1).astype(np.float64)
+
+    def f(x):
+        c, g, gh = O.compound_cost(x[:, :3 * n].reshape(E, n, 3), x[:, 3 * n:], w_area=1e-2, fixed_h=True)
+        return c, np.concatenate([g.reshape(E, -1), gh], 1)
+
+    t0 = time.perf_counter()
+    O.lbfgs(f, x0, max_iter=iters, history_size=history, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+    dt = time.perf_counter() - t0
+    return E / dt, O.num_threads(), dt
+
+
+# Algorithmic FP32 work per counted unit (flops; FMA = 2), from the kernel's
+# arithmetic: pair enumeration + centre cull, 16 piece AABB tests per near
+# pair, one piece-pair intersection area with both pose gradients, and the
+# L-BFGS two-loop per streamed history vector element.
+FLOPS_PER_PAIR = 6
+FLOPS_PER_NEAR = 128
+FLOPS_PER_PIECE_PAIR = 424
+FLOPS_PER_HIST_ELEM = 4
+FLOPS_PER_ITER_ELEM = 12
+
+
+def run_ours(args, rank, world, dev):
+    import torch
+
+    from packing_b200 import _lib
+    from packing_b200.cost import CostSpec
+    from packing_b200.lbfgs_torch_parallel import lbfgs
+    from packing_b200.relax import RelaxParams, relax_into, workspace_floats
+
+    E, n, iters, hist = args.E, args.n, args.iters, args.history
+    _lib.ensure_init(dev)
+    L = _lib.load()
+    xyt_np, h_np = workload(E, n, seed=rank)
+    xyt = torch.from_numpy(xyt_np).to(dev)
+    h = torch.from_numpy(h_np).to(dev)
+    xo = torch.empty_like(xyt)
+    ho = torch.empty_like(h)
+    loss = torch.empty(E, device=dev)
+    iters_out = torch.empty(E, dtype=torch.int32, device=dev)
+    work = torch.empty(workspace_floats([n] * E, hist), device=dev)
+    spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
+    prm = RelaxParams(n_iterations=iters, history_size=hist, max_step=0.01, final_eval=False)
+    flush = torch.empty(256 * 1024 * 1024 // 4, device=dev)   # > 126 MB L2
+    st = torch.cuda.current_stream(dev)
+
+    def step():
+        relax_into(xyt, h, xo, ho, loss, work, spec, prm, iters_out=iters_out)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    clk = ClockSampler(dev.index if rank == 0 else -1)
+    if rank == 0:
+        clk.start()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        step()
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    torch.cuda.synchronize(dev)
+    clocks = clk.stop() if rank == 0 else None
+    total = sum(times)
+    if world > 1:
+        t = torch.tensor([total], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total = float(t.item())
+        torch.distributed.barrier()
+    value = E * world * args.steps / total
+    ms_per_step = total / args.steps * 1e3
+    kernel_s = total / args.steps
+    assert torch.all(iters_out == iters), "an instance stopped early"
+    assert torch.isfinite(loss).all()
+
+    out = {"metric": METRIC, "value": value, "unit": "relaxations/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform poses, fixed square side)",
+           "config": {"workload": f"batched L-BFGS relaxation, fused one-launch form: E={E} packings x n={n} "
+                                  f"trees per GPU, history m={hist}, {iters} iterations, max_step 0.01, "
+                                  "cost boundary + overlap area, fixed h",
+                      "E_per_gpu": E, "n": n, "history": hist, "iterations": iters,
+                      "parallelism": f"instance sharding x{world}", "l2": "flushed between timed steps (256 MB write)"},
+           "gpu_launches": args.steps, "clocks": clocks}
+    if rank != 0 or args.quick:
+        return out if rank == 0 else None
+
+    # ---- e2e through the public API, pinned host buffers ----
+    xyt_host = torch.from_numpy(xyt_np).pin_memory()
+    h_host = torch.from_numpy(h_np).pin_memory()
+    xo_host = torch.empty_like(xyt_host).pin_memory()
+    loss_host = torch.empty(E).pin_memory()
+    e2e_times = []
+    for k in range(args.e2e_steps + 1):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        xd = xyt_host.to(dev, non_blocking=True)
+        hd = h_host.to(dev, non_blocking=True)
+        relax_into(xd, hd, xo, ho, loss, work, spec, prm)
+        xo_host.copy_(xo, non_blocking=True)
+        loss_host.copy_(loss, non_blocking=True)
+        e1.record(st)
+        e1.synchronize()
+        if k > 0:
+            e2e_times.append(e0.elapsed_time(e1) / 1e3)
+    e2e = E * len(e2e_times) / sum(e2e_times)
+    out["e2e"] = {"value": e2e, "unit": "relaxations/s", "h2d_bytes_per_step": xyt_host.numel() * 4 + h_host.numel() * 4,
+                  "d2h_bytes_per_step": xo_host.numel() * 4 + loss_host.numel() * 4}
+
+    # ---- roofline: counted work of the same launch, FP32 SIMT peak ----
+    counters = torch.zeros(6, dtype=torch.int64, device=dev)
+    prm_c = RelaxParams(n_iterations=iters, history_size=hist, max_step=0.01, final_eval=False, counters=counters)
+    relax_into(xyt, h, xo, ho, loss, work, spec, prm_c)
+    torch.cuda.synchronize(dev)
+    cnt = counters.cpu().numpy().astype(np.float64)
+    N = 3 * n + 3
+    flops = (cnt[0] * FLOPS_PER_PAIR + cnt[1] * FLOPS_PER_NEAR + cnt[2] * FLOPS_PER_PIECE_PAIR
+             + cnt[5] * FLOPS_PER_HIST_ELEM + cnt[4] * N * FLOPS_PER_ITER_ELEM)
+    peak = fp32_peak_tflops(torch, L, dev)
+    achieved = flops / kernel_s / 1e12
+    out["roofline"] = {"bound": "fp32_simt", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                       "frac": achieved / peak, "traffic": None,
+                       "peak_source": "measured FP32 FMA probe on this GPU (pk_fma_probe)",
+                       "work": {"pairs_enumerated": cnt[0], "near_pairs": cnt[1], "piece_pairs": cnt[2],
+                                "cost_evals": cnt[3], "iterations": cnt[4]}}
+
+    # ---- plain drop-in: the reference-style lbfgs loop over the cost kernel ----
+    if not args.skip_plain:
+        from packing_b200.cost import compound_cost
+        Ep = args.plain_E
+        gbuf = torch.empty((Ep, n, 3), device=dev)
+        ghbuf = torch.empty((Ep, 3), device=dev)
+        cbuf = torch.empty(Ep, device=dev)
+
+        def f(x, is_main):
+            compound_cost(x[:, :3 * n].reshape(Ep, n, 3), x[:, 3 * n:], spec, out_cost=cbuf, out_grad=gbuf,
+                          out_grad_h=ghbuf)
+            return cbuf, torch.cat([gbuf.reshape(Ep, -1), ghbuf], 1)
+
+        x0 = torch.cat([xyt[:Ep].reshape(Ep, -1), h[:Ep]], 1).contiguous()
+        x = x0.clone()
+        lbfgs(f, x, max_iter=3, history_size=hist, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+        torch.cuda.synchronize(dev)
+        x = x0.clone()
+        t0 = time.perf_counter()
+        lbfgs(f, x, max_iter=iters, history_size=hist, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+        torch.cuda.synchronize(dev)
+        pt = time.perf_counter() - t0
+        out["plain_dropin"] = {"value": Ep / pt, "unit": "relaxations/s", "E": Ep,
+                               "what": "packing_b200.lbfgs_torch_parallel.lbfgs (per-iteration launches, "
+                                       "host loop) over packing_b200.cost.compound_cost",
+                               "fused_over_plain": value / (Ep / pt)}
+
+    # ---- CPU baseline (oracle, host cores) ----
+    if not args.skip_cpu:
+        v, cores, dt = cpu_baseline_relax(args.cpu_E, n, iters, hist)
+        out["cpu_baseline"] = {"value": v, "unit": "relaxations/s", "cores": cores, "kind": "port",
+                               "sample": f"{args.cpu_E} packings x n={n}, {iters} iterations, m={hist} "
+                                         f"({dt:.1f} s, FP64 C oracle + numpy lbfgs restatement)"}
+    return out
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    O.lib()
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, cores, dt = cpu_baseline_relax(args.ref_E, args.n, args.iters, args.history, seed=1000 + k)
+        if k >= args.warmup:
+            vals.append((v, dt))
+    tot_t = sum(dt for _, dt in vals)
+    value = args.ref_E * len(vals) / tot_t
+    sample = (f"{args.ref_E} packings x n={args.n} per step, {args.iters} iterations, m={args.history}: FP64 C "
+              "restatement of the reference cost kernels + numpy restatement of its lbfgs, OpenMP over packings")
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "relaxations/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_t / len(vals) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded uniform poses, fixed square side)",
+            "config": {"workload": f"batched L-BFGS relaxation, n={args.n}, m={args.history}, {args.iters} iterations "
+                                   "(CPU sample of the per-GPU population)", "n": args.n},
+            "cpu_baseline": {"value": value, "unit": "relaxations/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "relaxations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--E", type=int, default=4096)
+    ap.add_argument("--n", type=int, default=200)
+    ap.add_argument("--iters", type=int, default=200)
+    ap.add_argument("--history", type=int, default=10)
+    ap.add_argument("--e2e-steps", dest="e2e_steps", type=int, default=2)
+    ap.add_argument("--plain-E", dest="plain_E", type=int, default=4096)
+    ap.add_argument("--cpu-E", dest="cpu_E", type=int, default=8)
+    ap.add_argument("--ref-E", dest="ref_E", type=int, default=4)
+    ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="headline timing only")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # CPU-only arm: rank 0 measures, the other ranks exit without work
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=dev)
+    out = run_ours(args, rank, world, dev)
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,216 @@
+/*
+ * packb200.h -- C ABI of the B200 (sm_100a) packing hot path.
+ *
+ * Every entry point returns an int status: PK_OK (0) on success, a negative
+ * PK_E* code otherwise, with a message readable through pk_last_error().
+ * Nothing here traps or aborts.  Pointers are device pointers unless a name
+ * says "host".  `stream` is a cudaStream_t passed as void* (NULL = legacy
+ * default stream).  All launches are asynchronous on that stream.
+ *
+ * Layouts (reference core/pack_cuda.py:1040-1064, 1186-1207):
+ *   xyt   float32 C-contiguous (E, n, 3) = [x, y, theta(rad)] per tree
+ *   h     float32 (E, 3) = [square side, x offset, y offset]
+ *   cost  float32 (E,)      grad float32 (E, n, 3)   grad_h float32 (E, 3)
+ * Ragged batches pack the trees of instance e at rows offsets[e] ..
+ * offsets[e+1]-1 of a (sum n, 3) array; offsets is int32 (E+1,).
+ *
+ * Outputs are caller-allocated and fully overwritten (no zeroing needed).
+ */
+#ifndef PACKB200_H
+#define PACKB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PK_OK 0
+#define PK_EINVAL -1      /* bad argument (shape, size, null pointer) */
+#define PK_ECUDA -2       /* CUDA runtime error */
+#define PK_ENOTINIT -3    /* pk_init not called on this device */
+#define PK_ERANGE -4      /* size beyond a documented maximum */
+
+#define PK_NUM_PIECES 4
+#define PK_MAX_TREE_VERTS 16
+#define PK_MAX_TREES 1024     /* trees per instance in the cost / relax kernels */
+#define PK_MAX_LAP_N 256      /* Hungarian matrix side (reference: 200) */
+
+/* Tree geometry: convex pieces (any orientation; the library makes them
+ * CCW as shapely.orient does, pack_cuda.py:824-826) and the outline used by
+ * the boundary cost.  Replaces kaggle_support.py:241-354 +
+ * pack_cuda.py:787-849 (_build_convex_piece_arrays). */
+typedef struct PkGeometry {
+    double piece_xy[PK_NUM_PIECES][4][2];
+    int piece_nv[PK_NUM_PIECES];          /* 3 or 4 */
+    double tree_xy[PK_MAX_TREE_VERTS][2];
+    int n_tree_verts;                     /* <= 16 */
+    double max_radius;                    /* max |vertex| of the outline */
+    double area;                          /* outline area (informational) */
+} PkGeometry;
+
+/* Fills *out with the reference Christmas tree (kaggle_support.py:241-324)
+ * for a given TREE_EXPANSION (kaggle_support.py:98 uses 20*(1.000001-1)),
+ * recentred on its centroid. */
+int pk_default_geometry(double tree_expansion, PkGeometry* out);
+
+/* Uploads the geometry to the current device; geom NULL = default tree.
+ * Must be called once per device before any compute call.  Replaces the
+ * lazy _ensure_initialized of pack_cuda.py:852-1032 (no runtime nvcc). */
+int pk_init(const PkGeometry* geom);
+
+/* Message of the last failing call on this host thread. */
+const char* pk_last_error(void);
+
+/* ---- cost and gradient (pack_cuda.py, pack_cuda_lut.py) --------------- */
+
+#define PK_PAIR_NONE 0
+#define PK_PAIR_AREA 1        /* overlap area,  CollisionCostOverlappingArea */
+#define PK_PAIR_SEP 2         /* sum of sep^2,  CollisionCostSeparation */
+#define PK_PAIR_LUT 3         /* LUT lookup,    pack_cuda_lut */
+
+/* LUT grid (pack_cuda_lut.py:30-86, constants :653-695).  vals is a device
+ * float32 (nx, ny, nt) C-order table over X (x >= one negative sample,
+ * mirrored), Y and theta. */
+typedef struct PkLut {
+    const float* vals;
+    int nx, ny, nt;
+    float x_min, x_max, y_min, y_max, t_min, t_max;
+    int quadratic;        /* apply max(0, v)^2 per pair */
+} PkLut;
+
+/* One fused pass per instance: total = w_area*h0^2 + w_boundary*boundary +
+ * w_pair*pairs, as CostCompound sums its terms (pack_cost.py:245-277).
+ * fixed_h zeroes grad_h (Cost.compute_cost, pack_cost.py:178-195). */
+typedef struct PkCostSpec {
+    int pair_mode;        /* PK_PAIR_* */
+    float w_pair;
+    float w_boundary;     /* 0 disables the boundary term (h may be NULL) */
+    float w_area;         /* AreaCost of a square: h0^2 (kaggle_support.py:803-816) */
+    int fixed_h;
+    PkLut lut;            /* used when pair_mode == PK_PAIR_LUT */
+} PkCostSpec;
+
+/* Compound cost over a uniform (offsets == NULL, all n_uniform trees) or
+ * ragged batch.  grad / grad_h may be NULL.  Deterministic: an instance's
+ * result does not depend on the rest of the batch.  No scratch memory.
+ * Replaces CostCompound.compute_cost over pack_cuda.overlap_multi_ensemble
+ * (pack_cuda.py:1040), boundary_distance_multi_ensemble (:1186) and
+ * pack_cuda_lut.overlap_multi_ensemble (pack_cuda_lut.py:783). */
+int pk_cost(const float* xyt, const int* offsets, int E, int n_uniform, const float* h,
+            const PkCostSpec* spec, float* cost, float* grad, float* grad_h, void* stream);
+
+/* pack_cuda.overlap_multi_ensemble(xyt, xyt, use_separation, out_cost,
+ * out_grads) (pack_cuda.py:1040-1183), non-periodic form. */
+int pk_overlap(const float* xyt, int E, int n, int use_separation, float* cost, float* grad,
+               void* stream);
+
+/* pack_cuda.boundary_distance_multi_ensemble (pack_cuda.py:1186-1295). */
+int pk_boundary(const float* xyt, const float* h, int E, int n, float* cost, float* grad,
+                float* grad_h, void* stream);
+
+/* pack_cuda_lut.overlap_multi_ensemble (pack_cuda_lut.py:783-862); ragged
+ * batches allowed through offsets. */
+int pk_overlap_lut(const float* xyt, const int* offsets, int E, int n_uniform, const PkLut* lut,
+                   float* cost, float* grad, void* stream);
+
+
+/* Fills vals (nx, ny, nt) with the analytic pair cost (PK_PAIR_AREA or
+ * PK_PAIR_SEP) of a tree at the origin against one at (X[ix], Y[iy], T[it])
+ * -- the LUT that CollisionCost._ensure_lut_initialized builds through
+ * LookupTable.build_from_function (pack_cost.py:322-377,
+ * pack_cuda_lut.py:90-169), evaluated on the GPU.  X, Y, T are device
+ * float32 vectors. */
+int pk_lut_build(const float* X, int nx, const float* Y, int ny, const float* T, int nt, int pair_mode,
+                 float* vals, void* stream);
+
+/* ---- batched linear assignment (lap_batch.py) ------------------------- */
+
+/* Hungarian on B float32 N x N matrices (solve_lap_batch with the default
+ * LAPConfig, lap_batch.py:457-534; kernel :62-165, totals :173-196).
+ * Assignments and totals are bit-identical to the reference's sequential
+ * kernel.  row_match int32 (B, N); total float32 (B,); status int32 (B,)
+ * nullable: 1 where a problem had no finite augmenting slack (rows -1,
+ * total NaN).  N <= 256.  No scratch memory. */
+int pk_lap_solve(const float* C, int B, int N, int* row_match, float* total, int* status, void* stream);
+
+/* Diversity between two sets of packings (compute_genetic_diversity_matrix,
+ * kaggle_support.py:2014-2129): for every (pop, ref) pair the minimum over
+ * the 8 symmetry transforms (transform != 0; else identity only) of the
+ * optimal assignment cost with entries sqrt(dx^2 + dy^2 + wrap(dtheta)^2).
+ * pop (Np, n, 3), ref (Nr, n, 3) float32; out (Np, Nr).  Cost rows are
+ * generated inside the assignment kernel; no (8 Np Nr, n, n) tensor. */
+int pk_diversity_matrix(const float* pop, const float* ref, int Np, int Nr, int n, int transform, float* out,
+                        void* stream);
+
+/* The (transforms * Np * Nr, n, n) cost matrices of the same computation
+ * in the reference's stacking order (kaggle_support.py:2118-2119). */
+int pk_diversity_costs(const float* pop, const float* ref, int Np, int Nr, int n, int transform, float* out,
+                       void* stream);
+
+/* compute_diversity_shortcut_kernel (lap_batch.py:537-607, kernel :216-331). */
+int pk_diversity_shortcut(const float* pop, const float* ref, int Np, int Nr, int n, float cos_a, float sin_a,
+                          int mirror, float* out, void* stream);
+
+/* ---- batched L-BFGS (lbfgs_torch_parallel.py) ------------------------- */
+
+/* One phase of one iteration of lbfgs (lbfgs_torch_parallel.py:411-729,
+ * line_search_fn=None) for M systems of N parameters, history m, while the
+ * objective stays with the caller.  arrays[17] = device pointers, in order:
+ * x, g, loss, d, prev_g, prev_loss, loss0 (M,N)/(M,) of the dtype;
+ * S, Y (M, m, N); ro (M, m); H, t (M,); hlen, hstart, evals, active (M,)
+ * int32; any_active (1,) int32.  dtype_bytes 4 (float32) or 8 (float64).
+ *   phase 0 init:      p0 = tolerance_grad
+ *   phase 1 direction: p0 = lr, p1 = max_step, i1 = has max_step, p2 = tolerance_change
+ *   phase 2 step:      x += t d
+ *   phase 3 update:    p0 = tolerance_grad, p1 = tolerance_change,
+ *                      p2 = tolerance_rel_change, i1 = stop_on_cost_increase, i2 = max_eval */
+int pk_lbfgs_phase(int phase, int dtype_bytes, void* const* arrays, int M, int N, int m, int n_iter, double p0,
+                   double p1, double p2, double p3, int i1, int i2, void* stream);
+
+typedef struct PkRelaxParams {
+    int max_iter;             /* n_iterations */
+    int history;              /* history_size, 1..64 */
+    float lr;
+    float max_step;
+    int has_max_step;
+    float tol_grad;           /* pack_dynamics passes 0 (pack_dynamics.py:127-137) */
+    float tol_change;         /* 0 there too */
+    float tol_rel_change;
+    int stop_on_cost_increase;
+    int max_eval;             /* reference default max_iter * 5 / 4 */
+    int final_eval;           /* 1: loss_out is the cost at the returned x */
+    unsigned long long* counters;  /* device (6,) or NULL: enumerated pairs, near pairs,
+                                      piece pairs, cost evaluations, iterations,
+                                      history entries streamed -- accumulated */
+} PkRelaxParams;
+
+/* Fused batched relaxation (OptimizerBFGS.run_simulation,
+ * pack_dynamics.py:54-149, over lbfgs :411-729): one launch relaxes every
+ * instance to max_iter with the compound cost of *spec, x = [xyt, h].
+ * Uniform (offsets NULL, n_max trees each) or ragged (offsets, n_max >= every
+ * size) batches; order (nullable) is a permutation of instances giving the
+ * launch order (largest first balances ragged batches).  xyt_out may alias
+ * xyt_in.  loss_out (E,) float32; iters_out (E,) int32 nullable.
+ * work: pk_relax_workspace_floats() floats of device scratch for the
+ * L-BFGS history.  An instance stops when it turns inactive, so its result
+ * does not depend on the rest of the batch. */
+int pk_relax(const float* xyt_in, const float* h_in, const int* offsets, const int* order, int E, int n_max,
+             const PkCostSpec* spec, const PkRelaxParams* params, float* xyt_out, float* h_out, float* loss_out,
+             int* iters_out, float* work, void* stream);
+
+/* Floats of work needed by pk_relax: sizes_host (E,) host int32 tree counts
+ * for a ragged batch, or NULL and n_uniform for a uniform one. */
+size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, int history);
+
+/* FP32 FMA throughput probe: blocks x threads x iters x 16 flops, for the
+ * roofline denominator of the SIMT-bound kernels. */
+int pk_fma_probe(float* out, int blocks, int threads, int iters, void* stream);
+
+int pk_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PACKB200_H */

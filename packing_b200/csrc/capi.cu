@@ -1,0 +1,35 @@
+// capi.cu -- the single translation unit of libpackb200.so.
+//
+// Every kernel family lives in a header included here so that the
+// __constant__ geometry tables are one symbol per loaded library.
+#include "common.cuh"
+#include "geometry.cuh"
+#include "cost.cuh"
+#include "lap.cuh"
+#include "lbfgs.cuh"
+
+extern "C" int pk_version(void) { return 1; }
+
+// Eight independent FMA chains per thread (16 flops per iteration).
+__global__ void pk_fma_probe_kernel(float* out, int iters)
+{
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = (float)(threadIdx.x + k) * 1e-3f;
+    const float b = 0.999999f, c = 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], b, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == 12345.678f) out[blockIdx.x] = s;   // keeps the chains alive
+}
+
+extern "C" int pk_fma_probe(float* out, int blocks, int threads, int iters, void* stream)
+{
+    if (blocks < 1 || threads < 1 || iters < 1 || !out) return pk_fail(PK_EINVAL, "pk_fma_probe: bad arguments%s");
+    pk_fma_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(out, iters);
+    return pk_cuda_check(cudaGetLastError(), "pk_fma_probe launch");
+}

@@ -1,0 +1,122 @@
+// common.cuh -- shared definitions for the packing_b200 CUDA library.
+//
+// The library is one translation unit (capi.cu includes every *.cuh), so the
+// __constant__ / __device__ symbols below exist once per loaded library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/packb200.h"
+
+#define PK_FULL_MASK 0xffffffffu
+
+// Tree geometry in the form the kernels read it.  Pieces are CCW; a
+// triangle is padded to four vertices as [v0, v1, v2, v0], so its edge 3 is
+// degenerate (zero length) and is skipped as a clipping line.
+struct PkDevGeom {
+    float2 piece[PK_NUM_PIECES][4];
+    int piece_nv[PK_NUM_PIECES];
+    float2 tree[PK_MAX_TREE_VERTS];
+    int n_tree;
+    float max_radius;
+    float cutoff_sq;    // (2 R)^2: farther centres cannot overlap
+};
+
+// FP64 copy for the legality validator.
+struct PkDevGeom64 {
+    double2 piece[PK_NUM_PIECES][4];
+    int piece_nv[PK_NUM_PIECES];
+    double2 tree[PK_MAX_TREE_VERTS];
+    int n_tree;
+    double max_radius;
+};
+
+__constant__ PkDevGeom c_geom;
+__constant__ PkDevGeom64 c_geom64;
+
+// Fixed-point scale of the pair-gradient accumulators: sums of int64 are
+// associative, so the result does not depend on the order in which threads
+// add their contributions (batched == single, bit for bit).
+#define PK_FX_SCALE 4294967296.0f          // 2^32
+#define PK_FX_INV (1.0 / 4294967296.0)
+
+__device__ __forceinline__ long long pk_to_fx(float v)
+{
+    return __float2ll_rn(v * PK_FX_SCALE);
+}
+
+__device__ __forceinline__ float pk_cross(float2 a, float2 b) { return a.x * b.y - a.y * b.x; }
+
+// (B - A) x (C - A): >= 0 means C is on or left of the directed line A->B.
+__device__ __forceinline__ float pk_cross3(float2 a, float2 b, float2 c)
+{
+    return (b.x - a.x) * (c.y - a.y) - (b.y - a.y) * (c.x - a.x);
+}
+
+template <typename T>
+__device__ __forceinline__ T pk_warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(PK_FULL_MASK, v, o);
+    return v;
+}
+
+// Deterministic block-wide sum: fixed warp-shuffle tree, then warp 0 sums the
+// per-warp partials in warp order.  scratch needs blockDim.x/32 entries.
+// Every thread gets the result.
+template <typename T>
+__device__ __forceinline__ T pk_block_sum(T v, T* scratch)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    v = pk_warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T r = (lane < nw) ? scratch[lane] : T(0);
+    if (warp == 0) {
+        r = pk_warp_sum(r);
+        if (lane == 0) scratch[0] = r;
+    }
+    __syncthreads();
+    r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T pk_block_max(T v, T* scratch)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(PK_FULL_MASK, v, o));
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T r = (lane < nw) ? scratch[lane] : scratch[0];
+    if (warp == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r = max(r, __shfl_xor_sync(PK_FULL_MASK, r, o));
+        if (lane == 0) scratch[0] = r;
+    }
+    __syncthreads();
+    r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+// Bounded wrap of an angle difference into [-pi, pi], following the
+// reference's subtract-2pi loop (pack_cuda_lut.py:289-293) in FP32.  Angles
+// beyond +-64 pi are reduced with remainderf first so the loop stays short.
+__device__ __forceinline__ float pk_wrap_angle(float t)
+{
+    const float PI = 3.14159265358979323846f;
+    if (!(fabsf(t) < 64.0f * PI)) t = remainderf(t, 2.0f * PI);
+    while (t > PI) t -= 2.0f * PI;
+    while (t < -PI) t += 2.0f * PI;
+    return t;
+}

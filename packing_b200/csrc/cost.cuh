@@ -1,0 +1,799 @@
+// cost.cuh -- batched tree-pair + boundary cost and gradient.
+//
+// One CTA evaluates one packing (instance).  Work per instance:
+//   phase 0  thread per tree: pose -> (x, y, cos, sin), piece AABBs relative to
+//            the tree centre, and the boundary term (pack_cuda.py:550-642).
+//   phase A  every unordered pair {i, j} once (not both orders as the
+//            reference's 2-threads-per-ref-tree loop does, pack_cuda.py:404-464),
+//            centre cull at (2R)^2, then the 16 piece-pair AABB tests; the
+//            surviving piece pairs are appended to a shared-memory work list
+//            (warp ballot + one shared atomic per warp).
+//   phase B  thread per listed piece pair: intersection area (or SAT
+//            penetration) with the gradient of BOTH trees' poses, added into
+//            per-tree int64 fixed-point accumulators (order-independent, so
+//            deterministic), flushed whenever the list fills.
+//   phase C  per-tree gradients out; totals by fixed-order reductions.
+// Coordinates are taken relative to tree i's centre so the clipper works on
+// O(1) numbers whatever the packing's extent.
+#pragma once
+#include "common.cuh"
+
+struct PkCostSmem {
+    float4* pose;       // [n_max] x, y, cos, sin
+    float* theta;       // [n_max]
+    float4* aabb;       // [4*n_max] per piece: minx, maxx, miny, maxy (centre-relative)
+    long long* acc;     // [3*n_max] fixed-point gradient
+    float4* bnd;        // [n_max] boundary: cost, dh0, dh1, dh2 (unweighted)
+    uint32_t* items;    // [cap]
+    int* count;
+    double* red;        // [32]
+    long long* redl;    // [32]
+    float2* piece;      // [16]
+    int* piece_nv;      // [4]
+    unsigned int* cnt;  // [4] enumerated pairs, near pairs, piece pairs, evaluations
+    int cap;
+};
+
+__host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap)
+{
+    size_t b = 0;
+    b += (size_t)n_max * 16;        // pose
+    b += (size_t)n_max * 16;        // bnd
+    b += (size_t)n_max * 64;        // aabb
+    b += (size_t)n_max * 24;        // acc
+    b += (size_t)n_max * 4;         // theta
+    b += (size_t)cap * 4;           // items
+    b += 32 * 8 + 32 * 8 + 16 * 8 + 4 * 4 + 16 + 16;
+    return b;
+}
+
+__device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int cap)
+{
+    PkCostSmem s;
+    unsigned char* p = base;
+    s.pose = (float4*)p; p += (size_t)n_max * 16;
+    s.bnd = (float4*)p; p += (size_t)n_max * 16;
+    s.aabb = (float4*)p; p += (size_t)n_max * 64;
+    s.acc = (long long*)p; p += (size_t)n_max * 24;
+    s.red = (double*)p; p += 32 * 8;
+    s.redl = (long long*)p; p += 32 * 8;
+    s.piece = (float2*)p; p += 16 * 8;
+    s.theta = (float*)p; p += (size_t)n_max * 4;
+    s.items = (uint32_t*)p; p += (size_t)cap * 4;
+    s.piece_nv = (int*)p; p += 16;
+    s.count = (int*)p; p += 16;
+    s.cnt = (unsigned int*)p; p += 16;
+    s.cap = cap;
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Convex piece intersection area with the gradient of both rigid poses.
+//
+// The reference clips the subject piece against the clip piece edge by edge
+// (Sutherland-Hodgman, pack_cuda_primitives.py:238-296, 348-538) and back-
+// propagates through every stage for the subject's vertex gradient.  Here the
+// same area is assembled from the boundary of P n Q directly: each edge of P
+// is clipped to the part inside Q (parametric interval against Q's half-
+// planes, inside = cross >= 0 as in :263-264) and each edge of Q to the part
+// inside P.  With both pieces CCW, the area is sum 1/2 cross(a', b') over
+// those portions (Green's theorem).  A rigid motion of P moves only the P
+// portions, so dA/d(x, y) = sum of their outward normals N = len * n_hat and
+// dA/dtheta = sum cross(midpoint - centre, N) (exact for straight edges).
+// Collinear edges: a P edge lying on a Q edge line is excluded; a Q edge on a
+// P edge line is kept only if both run the same way, so a shared boundary
+// segment is counted once and touching pieces contribute zero.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_tri,
+                                                   const float2 (&Q)[4], bool q_tri, float2 d,
+                                                   float& area, float3& gP, float3& gQ)
+{
+    float fPQ[4][4];   // [Q line k][P vertex v]
+    float fQP[4][4];   // [P line k][Q vertex v]
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 qa = Q[k], qb = Q[(k + 1) & 3];
+        const float2 pa = P[k], pb = P[(k + 1) & 3];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            fPQ[k][v] = pk_cross3(qa, qb, P[v]);
+            fQP[k][v] = pk_cross3(pa, pb, Q[v]);
+        }
+    }
+    float A2 = 0.f;   // twice the area
+    gP = make_float3(0.f, 0.f, 0.f);
+    gQ = make_float3(0.f, 0.f, 0.f);
+    // Edges of P against Q's half-planes.
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        if (v == 3 && p_tri) continue;
+        const float2 a = P[v], b = P[(v + 1) & 3];
+        float tin = 0.f, tout = 1.f;
+        bool empty = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k == 3 && q_tri) continue;
+            const float fa = fPQ[k][v], fb = fPQ[k][(v + 1) & 3];
+            const bool ia = fa >= 0.f, ib = fb >= 0.f;
+            if (!ia && !ib) {
+                empty = true;
+            } else if (ia && ib) {
+                if (fa == 0.f && fb == 0.f) empty = true;
+            } else {
+                const float t = fa / (fa - fb);
+                if (ia) tout = fminf(tout, t);
+                else tin = fmaxf(tin, t);
+            }
+        }
+        if (!empty && tin < tout) {
+            const float dt = tout - tin;
+            const float2 e = make_float2(b.x - a.x, b.y - a.y);
+            A2 += dt * pk_cross(a, b);
+            const float2 N = make_float2(dt * e.y, -dt * e.x);
+            const float tm = 0.5f * (tin + tout);
+            const float2 m = make_float2(a.x + tm * e.x, a.y + tm * e.y);
+            gP.x += N.x;
+            gP.y += N.y;
+            gP.z += pk_cross(m, N);
+        }
+    }
+    // Edges of Q against P's half-planes.
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        if (v == 3 && q_tri) continue;
+        const float2 a = Q[v], b = Q[(v + 1) & 3];
+        const float2 e = make_float2(b.x - a.x, b.y - a.y);
+        float tin = 0.f, tout = 1.f;
+        bool empty = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k == 3 && p_tri) continue;
+            const float fa = fQP[k][v], fb = fQP[k][(v + 1) & 3];
+            const bool ia = fa >= 0.f, ib = fb >= 0.f;
+            if (!ia && !ib) {
+                empty = true;
+            } else if (ia && ib) {
+                if (fa == 0.f && fb == 0.f) {
+                    const float2 pe = make_float2(P[(k + 1) & 3].x - P[k].x, P[(k + 1) & 3].y - P[k].y);
+                    if (pe.x * e.x + pe.y * e.y <= 0.f) empty = true;
+                }
+            } else {
+                const float t = fa / (fa - fb);
+                if (ia) tout = fminf(tout, t);
+                else tin = fmaxf(tin, t);
+            }
+        }
+        if (!empty && tin < tout) {
+            const float dt = tout - tin;
+            A2 += dt * pk_cross(a, b);
+            const float2 N = make_float2(dt * e.y, -dt * e.x);
+            const float tm = 0.5f * (tin + tout);
+            const float2 m = make_float2(a.x + tm * e.x - d.x, a.y + tm * e.y - d.y);
+            gQ.x += N.x;
+            gQ.y += N.y;
+            gQ.z += pk_cross(m, N);
+        }
+    }
+    area = 0.5f * A2;
+    if (!(area > 0.f)) {   // empty or numerically vanishing overlap
+        area = 0.f;
+        gP = make_float3(0.f, 0.f, 0.f);
+        gQ = make_float3(0.f, 0.f, 0.f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// SAT penetration depth (sat_separation_with_grad_pose,
+// pack_cuda_primitives.py:544-828) with the pose gradient of both pieces.
+// Axes: P's edge normals, then Q's; a separating axis returns 0; the
+// smallest overlap wins (strict <), pen1 <= pen2 selects case 1.  The
+// reference evaluates each ordered pair and keeps the ref gradient; the
+// other piece's gradient here is the same expression with the roles swapped
+// (translation: the negative; rotation: its own extreme vertex, plus the
+// axis-rotation term when the axis is one of its edges).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pk_piece_sat_grad(const float2 (&P)[4], bool p_tri, const float2 (&Q)[4],
+                                                  bool q_tri, float2 d, float& sep, float3& gP,
+                                                  float3& gQ)
+{
+    sep = 0.f;
+    gP = make_float3(0.f, 0.f, 0.f);
+    gQ = make_float3(0.f, 0.f, 0.f);
+    float best = 1.0e30f;
+    bool found = false, from1 = false;
+    float sigma = 1.f;
+    float2 bn = make_float2(0.f, 0.f), bv = bn, bw = bn;
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool tri = pass == 0 ? p_tri : q_tri;
+            if (k == 3 && tri) continue;
+            const float2 a = pass == 0 ? P[k] : Q[k];
+            const float2 b = pass == 0 ? P[(k + 1) & 3] : Q[(k + 1) & 3];
+            float2 nr = make_float2(-(b.y - a.y), b.x - a.x);
+            const float len = sqrtf(nr.x * nr.x + nr.y * nr.y);
+            if (len < 1.0e-12f) continue;
+            nr.x /= len;
+            nr.y /= len;
+            float p1[4], p2[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                p1[v] = P[v].x * nr.x + P[v].y * nr.y;
+                p2[v] = Q[v].x * nr.x + Q[v].y * nr.y;
+            }
+            float mn1 = p1[0], mx1 = p1[0], mn2 = p2[0], mx2 = p2[0];
+#pragma unroll
+            for (int v = 1; v < 4; ++v) {
+                mn1 = fminf(mn1, p1[v]); mx1 = fmaxf(mx1, p1[v]);
+                mn2 = fminf(mn2, p2[v]); mx2 = fmaxf(mx2, p2[v]);
+            }
+            if (mx1 < mn2 || mx2 < mn1) return;   // separating axis: no overlap
+            found = true;
+            const float pen1 = mx1 - mn2, pen2 = mx2 - mn1;
+            const float pen = pen1 < pen2 ? pen1 : pen2;
+            if (pen < best) {
+                best = pen;
+                bn = nr;
+                from1 = pass == 0;
+                const bool c1 = pen1 <= pen2;
+                sigma = c1 ? 1.f : -1.f;
+                // first vertex attaining the extreme, like the reference scans
+                float2 v = P[0], w = Q[0];
+                float pv = p1[0], pw = p2[0];
+#pragma unroll
+                for (int q = 1; q < 4; ++q) {
+                    if (c1 ? (p1[q] > pv) : (p1[q] < pv)) { pv = p1[q]; v = P[q]; }
+                    if (c1 ? (p2[q] < pw) : (p2[q] > pw)) { pw = p2[q]; w = Q[q]; }
+                }
+                bv = v;
+                bw = w;
+            }
+        }
+    }
+    if (!found || best <= 1.0e-12f) return;
+    sep = best;
+    const float2 gv = make_float2(sigma * bn.x, sigma * bn.y);
+    const float2 rn = make_float2(-bn.y, bn.x);                     // d n / d theta
+    const float2 vw = make_float2(bv.x - bw.x, bv.y - bw.y);
+    const float axis_term = sigma * (vw.x * rn.x + vw.y * rn.y);
+    const float2 rq = make_float2(bw.x - d.x, bw.y - d.y);
+    gP.x = gv.x;
+    gP.y = gv.y;
+    gP.z = gv.x * -bv.y + gv.y * bv.x + (from1 ? axis_term : 0.f);
+    gQ.x = -gv.x;
+    gQ.y = -gv.y;
+    gQ.z = -(gv.x * -rq.y + gv.y * rq.x) + (from1 ? 0.f : axis_term);
+}
+
+// ---------------------------------------------------------------------------
+// LUT lookup with analytic gradient (lut_lookup_with_grad,
+// pack_cuda_lut.py:298-415), FP32 with the reference's operation order.
+// Indices are clamped into the table (the reference can read one cell out of
+// range when a trimmed theta range is mirrored).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float pk_lut_lookup(const PkLut& L, float x, float y, float th, float3& g)
+{
+    g = make_float3(0.f, 0.f, 0.f);
+    if (x < -L.x_max || x > L.x_max || y < L.y_min || y > L.y_max || th < L.t_min || th > L.t_max)
+        return 0.f;
+    const float xt = x >= 0.f ? x : -x;
+    const float tt = x >= 0.f ? th : -th;
+    const float gx = (xt - L.x_min) / (L.x_max - L.x_min) * (float)(L.nx - 1);
+    const float gy = (y - L.y_min) / (L.y_max - L.y_min) * (float)(L.ny - 1);
+    const float gt = (tt - L.t_min) / (L.t_max - L.t_min) * (float)(L.nt - 1);
+    int ix0 = (int)floorf(gx), iy0 = (int)floorf(gy), it0 = (int)floorf(gt);
+    const float fx = gx - ix0, fy = gy - iy0, ft = gt - it0;
+    ix0 = min(max(ix0, 0), L.nx - 1);
+    iy0 = min(max(iy0, 0), L.ny - 1);
+    it0 = min(max(it0, 0), L.nt - 1);
+    const int ix1 = min(ix0 + 1, L.nx - 1), iy1 = min(iy0 + 1, L.ny - 1), it1 = min(it0 + 1, L.nt - 1);
+    const size_t sy = (size_t)L.nt, sx = (size_t)L.ny * L.nt;
+    const float* V = L.vals;
+    const float v000 = __ldg(V + ix0 * sx + iy0 * sy + it0), v001 = __ldg(V + ix0 * sx + iy0 * sy + it1);
+    const float v010 = __ldg(V + ix0 * sx + iy1 * sy + it0), v011 = __ldg(V + ix0 * sx + iy1 * sy + it1);
+    const float v100 = __ldg(V + ix1 * sx + iy0 * sy + it0), v101 = __ldg(V + ix1 * sx + iy0 * sy + it1);
+    const float v110 = __ldg(V + ix1 * sx + iy1 * sy + it0), v111 = __ldg(V + ix1 * sx + iy1 * sy + it1);
+    const float v00 = v000 * (1.0f - ft) + v001 * ft, v01 = v010 * (1.0f - ft) + v011 * ft;
+    const float v10 = v100 * (1.0f - ft) + v101 * ft, v11 = v110 * (1.0f - ft) + v111 * ft;
+    const float v0 = v00 * (1.0f - fy) + v01 * fy, v1 = v10 * (1.0f - fy) + v11 * fy;
+    const float val = v0 * (1.0f - fx) + v1 * fx;
+    const float dfx = v1 - v0;
+    const float dfy = (1.0f - fx) * (v01 - v00) + fx * (v11 - v10);
+    const float d0 = (v001 - v000) * (1.0f - fy) + (v011 - v010) * fy;
+    const float d1 = (v101 - v100) * (1.0f - fy) + (v111 - v110) * fy;
+    const float dft = d0 * (1.0f - fx) + d1 * fx;
+    g.x = dfx * ((float)(L.nx - 1) / (L.x_max - L.x_min));
+    g.y = dfy * ((float)(L.ny - 1) / (L.y_max - L.y_min));
+    g.z = dft * ((float)(L.nt - 1) / (L.t_max - L.t_min));
+    if (x < 0.f) { g.x = -g.x; g.z = -g.z; }
+    return val;
+}
+
+__device__ __forceinline__ void pk_acc_add(long long* acc, int t, float3 g)
+{
+    atomicAdd((unsigned long long*)&acc[3 * t + 0], (unsigned long long)pk_to_fx(g.x));
+    atomicAdd((unsigned long long*)&acc[3 * t + 1], (unsigned long long)pk_to_fx(g.y));
+    atomicAdd((unsigned long long*)&acc[3 * t + 2], (unsigned long long)pk_to_fx(g.z));
+}
+
+__device__ __forceinline__ void pk_load_piece(const PkCostSmem& sm, int p, float c, float s, float ox,
+                                              float oy, float2 (&V)[4])
+{
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const float2 l = sm.piece[p * 4 + v];
+        V[v] = make_float2(c * l.x - s * l.y + ox, s * l.x + c * l.y + oy);
+    }
+}
+
+// Phase B: evaluate every listed item; returns this thread's fixed-point
+// pair total.  Items: i (11 bits) | j (11 bits) | pi (2) | pj (2).
+template <int MODE>
+__device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, int count, float w_pair,
+                                                      const PkLut& lut)
+{
+    long long tot = 0;
+    for (int w = threadIdx.x; w < count; w += blockDim.x) {
+        const uint32_t it = sm.items[w];
+        const int i = it & 2047, j = (it >> 11) & 2047;
+        const float4 A = sm.pose[i], B = sm.pose[j];
+        const float2 d = make_float2(B.x - A.x, B.y - A.y);
+        float val;
+        float3 gi, gj;
+        if (MODE == PK_PAIR_LUT) {
+            // ref = lower index, as the reference's triangular loop (pack_cuda_lut.py:437)
+            const int r = i < j ? i : j, o = i < j ? j : i;
+            const float4 R = sm.pose[r], O = sm.pose[o];
+            const float dxw = O.x - R.x, dyw = O.y - R.y;
+            const float dxl = R.z * dxw + R.w * dyw;
+            const float dyl = -R.w * dxw + R.z * dyw;
+            const float dth = pk_wrap_angle(sm.theta[o] - sm.theta[r]);
+            float3 gl;
+            val = pk_lut_lookup(lut, dxl, dyl, dth, gl);
+            if (lut.quadratic) {
+                if (val > 0.f) {
+                    gl.x *= 2.0f * val; gl.y *= 2.0f * val; gl.z *= 2.0f * val;
+                    val = val * val;
+                } else {
+                    val = 0.f;
+                    gl = make_float3(0.f, 0.f, 0.f);
+                }
+            }
+            float3 gr = make_float3(-gl.x * R.z + gl.y * R.w, -gl.x * R.w - gl.y * R.z,
+                                    gl.x * dyl - gl.y * dxl - gl.z);
+            float3 go = make_float3(gl.x * R.z - gl.y * R.w, gl.x * R.w + gl.y * R.z, gl.z);
+            gi = (r == i) ? gr : go;
+            gj = (r == i) ? go : gr;
+        } else {
+            const int pi = (it >> 22) & 3, pj = (it >> 24) & 3;
+            float2 P[4], Q[4];
+            pk_load_piece(sm, pi, A.z, A.w, 0.f, 0.f, P);
+            pk_load_piece(sm, pj, B.z, B.w, d.x, d.y, Q);
+            const bool pt = sm.piece_nv[pi] == 3, qt = sm.piece_nv[pj] == 3;
+            if (MODE == PK_PAIR_AREA) {
+                pk_piece_area_grad(P, pt, Q, qt, d, val, gi, gj);
+            } else {
+                float sp;
+                pk_piece_sat_grad(P, pt, Q, qt, d, sp, gi, gj);
+                const float f = 2.0f * sp;
+                gi = make_float3(f * gi.x, f * gi.y, f * gi.z);
+                gj = make_float3(f * gj.x, f * gj.y, f * gj.z);
+                val = sp * sp;
+            }
+        }
+        if (val != 0.f || gi.x != 0.f || gi.y != 0.f || gi.z != 0.f) {
+            tot += pk_to_fx(w_pair * val);
+            pk_acc_add(sm.acc, i, make_float3(w_pair * gi.x, w_pair * gi.y, w_pair * gi.z));
+            pk_acc_add(sm.acc, j, make_float3(w_pair * gj.x, w_pair * gj.y, w_pair * gj.z));
+        }
+    }
+    return tot;
+}
+
+// Sum of v[0..n) in an order fixed by n alone (not by blockDim): lane l of
+// warp 0 adds its contiguous chunk, then a fixed shuffle tree.  Called by all
+// threads; returns the sum to all.
+template <typename F>
+__device__ __forceinline__ double pk_canonical_sum(int n, F get, double* red)
+{
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        const int k = (n + 31) >> 5;
+        const int b = threadIdx.x * k, e = min(n, b + k);
+        for (int t = b; t < e; ++t) s += get(t);
+        s = pk_warp_sum(s);
+        if (threadIdx.x == 0) red[0] = s;
+    }
+    __syncthreads();
+    s = red[0];
+    __syncthreads();
+    return s;
+}
+
+struct PkEvalOut {
+    double cost;
+};
+
+// Evaluate one instance.  X: 3n floats (global or shared), H: 3 floats or
+// NULL.  G: 3n floats or NULL (written, not accumulated); GH: 3 floats or
+// NULL.  Must be called by every thread of the block.
+template <int MODE>
+__device__ double pk_eval_instance(const float* X, int n, const float* H, const PkCostSpec& spec,
+                                   float* G, float* GH, const PkCostSmem& sm)
+{
+    const int T = blockDim.x;
+    const bool do_bnd = spec.w_boundary != 0.f && H != nullptr;
+    float half = 0.f, hox = 0.f, hoy = 0.f;
+    if (H) { half = H[0] * 0.5f; hox = H[1]; hoy = H[2]; }
+    // ---- phase 0: per tree -------------------------------------------------
+    for (int t = threadIdx.x; t < n; t += T) {
+        const float x = X[3 * t], y = X[3 * t + 1], th = X[3 * t + 2];
+        float s, c;
+        sincosf(th, &s, &c);
+        sm.pose[t] = make_float4(x, y, c, s);
+        sm.theta[t] = th;
+        long long a0 = 0, a1 = 0, a2 = 0;
+        float4 bnd = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (MODE == PK_PAIR_AREA || MODE == PK_PAIR_SEP) {
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                float2 V[4];
+                pk_load_piece(sm, p, c, s, 0.f, 0.f, V);
+                float4 bb = make_float4(V[0].x, V[0].x, V[0].y, V[0].y);
+#pragma unroll
+                for (int v = 1; v < 4; ++v) {
+                    bb.x = fminf(bb.x, V[v].x); bb.y = fmaxf(bb.y, V[v].x);
+                    bb.z = fminf(bb.z, V[v].y); bb.w = fmaxf(bb.w, V[v].y);
+                }
+                const float eps = 1e-6f;
+                sm.aabb[4 * t + p] = make_float4(bb.x - eps, bb.y + eps, bb.z - eps, bb.w + eps);
+            }
+        }
+        if (do_bnd) {
+            // boundary_distance_tree, pack_cuda.py:550-642
+            float best = 0.f;
+            int bi = 0;
+            for (int v = 0; v < c_geom.n_tree; ++v) {
+                const float2 l = c_geom.tree[v];
+                const float vx = c * l.x - s * l.y + x - hox;
+                const float vy = s * l.x + c * l.y + y - hoy;
+                const float ax = fabsf(vx), ay = fabsf(vy);
+                const float dx = ax > half ? ax - half : 0.f;
+                const float dy = ay > half ? ay - half : 0.f;
+                const float dd = dx * dx + dy * dy;
+                if (dd > best) { best = dd; bi = v; }
+            }
+            const float2 l = c_geom.tree[bi];
+            const float vx = c * l.x - s * l.y + x - hox;
+            const float vy = s * l.x + c * l.y + y - hoy;
+            const float ax = fabsf(vx), ay = fabsf(vy);
+            const float dx = ax > half ? ax - half : 0.f;
+            const float dy = ay > half ? ay - half : 0.f;
+            const float gvx = dx > 0.f ? 2.0f * dx * (vx >= 0.f ? 1.f : -1.f) : 0.f;
+            const float gvy = dy > 0.f ? 2.0f * dy * (vy >= 0.f ? 1.f : -1.f) : 0.f;
+            const float gth = gvx * (-s * l.x - c * l.y) + gvy * (c * l.x - s * l.y);
+            const float wb = spec.w_boundary;
+            a0 = pk_to_fx(wb * gvx);
+            a1 = pk_to_fx(wb * gvy);
+            a2 = pk_to_fx(wb * gth);
+            bnd = make_float4(best, -(dx + dy), -gvx, -gvy);
+        }
+        sm.acc[3 * t] = a0;
+        sm.acc[3 * t + 1] = a1;
+        sm.acc[3 * t + 2] = a2;
+        sm.bnd[t] = bnd;
+    }
+    if (threadIdx.x < 16) sm.piece[threadIdx.x] = c_geom.piece[threadIdx.x >> 2][threadIdx.x & 3];
+    if (threadIdx.x < 4) sm.piece_nv[threadIdx.x] = c_geom.piece_nv[threadIdx.x];
+    if (threadIdx.x == 0) {
+        *sm.count = 0;
+        sm.cnt[3] += 1;
+        if (MODE != PK_PAIR_NONE && n > 1) sm.cnt[0] += (unsigned)(n * (n - 1) / 2);
+    }
+    __syncthreads();
+
+    // ---- phases A + B: pairs -------------------------------------------------
+    long long pair_tot = 0;
+    if (MODE != PK_PAIR_NONE && n > 1) {
+        const int npairs = n * (n - 1) / 2;
+        const float cutoff = c_geom.cutoff_sq;
+        const int lane = threadIdx.x & 31;
+        const int per_round = (MODE == PK_PAIR_LUT) ? T : 16 * T;
+        for (int base = 0; base < npairs; base += T) {
+            const int k = base + threadIdx.x;
+            uint32_t mask = 0;
+            int i = 0, j = 0;
+            if (k < npairs) {
+                // pair k: distance class dd = k / n + 1, i = k mod n, j = (i + dd) mod n
+                const int dd = k / n;
+                i = k - dd * n;
+                j = i + dd + 1;
+                if (j >= n) j -= n;
+                const float4 A = sm.pose[i], B = sm.pose[j];
+                const float dx = B.x - A.x, dy = B.y - A.y;
+                if (dx * dx + dy * dy <= cutoff) {
+                    if (MODE == PK_PAIR_LUT) {
+                        mask = 1;
+                    } else {
+#pragma unroll
+                        for (int p = 0; p < 4; ++p) {
+                            const float4 a = sm.aabb[4 * i + p];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                const float4 b = sm.aabb[4 * j + q];
+                                const bool ov = !(a.y < b.x + dx || b.y + dx < a.x || a.w < b.z + dy ||
+                                                  b.w + dy < a.z);
+                                mask |= (uint32_t)ov << (4 * p + q);
+                            }
+                        }
+                    }
+                }
+            }
+            const int cnt = __popc(mask);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(PK_FULL_MASK, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int wtot = __shfl_sync(PK_FULL_MASK, incl, 31);
+            const unsigned nnear = __popc(__ballot_sync(PK_FULL_MASK, mask != 0));
+            int wbase = 0;
+            if (lane == 31 && wtot) {
+                wbase = atomicAdd(sm.count, wtot);
+                atomicAdd(&sm.cnt[1], nnear);
+                atomicAdd(&sm.cnt[2], (unsigned)wtot);
+            }
+            wbase = __shfl_sync(PK_FULL_MASK, wbase, 31);
+            int pos = wbase + incl - cnt;
+            const uint32_t ij = (uint32_t)i | ((uint32_t)j << 11);
+            while (mask) {
+                const int b = __ffs(mask) - 1;
+                mask &= mask - 1;
+                sm.items[pos++] = ij | ((uint32_t)(b >> 2) << 22) | ((uint32_t)(b & 3) << 24);
+            }
+            __syncthreads();
+            const int count = *sm.count;
+            if (count > sm.cap - per_round || base + T >= npairs) {
+                pair_tot += pk_process_items<MODE>(sm, count, spec.w_pair, spec.lut);
+                __syncthreads();
+                if (threadIdx.x == 0) *sm.count = 0;
+                __syncthreads();
+            }
+        }
+    }
+
+    // ---- phase C: outputs ----------------------------------------------------
+    if (G) {
+        for (int t = threadIdx.x; t < n; t += T) {
+            G[3 * t] = (float)((double)sm.acc[3 * t] * PK_FX_INV);
+            G[3 * t + 1] = (float)((double)sm.acc[3 * t + 1] * PK_FX_INV);
+            G[3 * t + 2] = (float)((double)sm.acc[3 * t + 2] * PK_FX_INV);
+        }
+    }
+    const long long ptot = pk_block_sum<long long>(pair_tot, sm.redl);
+    double total = (double)ptot * PK_FX_INV;
+    double h0 = H ? (double)H[0] : 0.0;
+    if (do_bnd) {
+        const double bsum = pk_canonical_sum(n, [&](int t) { return (double)sm.bnd[t].x; }, sm.red);
+        total += (double)spec.w_boundary * bsum;
+        if (GH) {
+            const double g0 = pk_canonical_sum(n, [&](int t) { return (double)sm.bnd[t].y; }, sm.red);
+            const double g1 = pk_canonical_sum(n, [&](int t) { return (double)sm.bnd[t].z; }, sm.red);
+            const double g2 = pk_canonical_sum(n, [&](int t) { return (double)sm.bnd[t].w; }, sm.red);
+            if (threadIdx.x == 0) {
+                GH[0] = (float)(spec.w_boundary * g0 + (double)spec.w_area * 2.0 * h0);
+                GH[1] = (float)(spec.w_boundary * g1);
+                GH[2] = (float)(spec.w_boundary * g2);
+            }
+        }
+    } else if (GH && threadIdx.x == 0) {
+        GH[0] = (float)((double)spec.w_area * 2.0 * h0);
+        GH[1] = 0.f;
+        GH[2] = 0.f;
+    }
+    if (GH && spec.fixed_h && threadIdx.x == 0) { GH[0] = 0.f; GH[1] = 0.f; GH[2] = 0.f; }
+    total += (double)spec.w_area * h0 * h0;
+    __syncthreads();
+    return total;
+}
+
+template <int MODE>
+__global__ void pk_cost_kernel(const float* __restrict__ xyt, const int* __restrict__ offsets, int E,
+                               int n_max, const float* __restrict__ h, PkCostSpec spec,
+                               float* __restrict__ cost, float* __restrict__ grad,
+                               float* __restrict__ grad_h, int cap)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    const int e = blockIdx.x;
+    if (e >= E) return;
+    const int base = offsets ? offsets[e] : e * n_max;
+    const int n = offsets ? offsets[e + 1] - base : n_max;
+    if (n < 0 || n > n_max) {
+        if (threadIdx.x == 0) cost[e] = __int_as_float(0x7fc00000);   // NaN marks a bad offset
+        return;
+    }
+    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap);
+    if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const double tot = pk_eval_instance<MODE>(xyt + (size_t)base * 3, n, h ? h + 3 * e : nullptr, spec,
+                                              grad ? grad + (size_t)base * 3 : nullptr,
+                                              grad_h ? grad_h + 3 * e : nullptr, sm);
+    if (threadIdx.x == 0) cost[e] = (float)tot;
+}
+
+// Threads per CTA as a function of the instance size only (so a packing's
+// result never depends on what else is in the batch).
+static inline int pk_cost_threads(int n_max)
+{
+    if (n_max <= 48) return 64;
+    if (n_max <= 128) return 128;
+    return 256;
+}
+
+// Item-list capacity: one round appends at most T (LUT) or 16 T items and the
+// list is flushed before it could overflow, so cap must exceed that bound.
+static inline int pk_cost_cap(int T, int mode) { return mode == PK_PAIR_LUT ? 4 * T : 24 * T; }
+
+static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max, const float* h,
+                          const PkCostSpec* spec, float* cost, float* grad, float* grad_h,
+                          cudaStream_t st)
+{
+    int rc = pk_check_init();
+    if (rc) return rc;
+    if (!spec) return pk_fail(PK_EINVAL, "pk_cost: spec is NULL%s");
+    if (E < 0 || n_max < 0) return pk_fail(PK_EINVAL, "pk_cost: negative size%s");
+    if (E == 0) return PK_OK;
+    if (n_max > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_cost: more than 1024 trees per instance%s");
+    if (!xyt || !cost) return pk_fail(PK_EINVAL, "pk_cost: xyt and cost are required%s");
+    if (spec->w_boundary != 0.f && !h) return pk_fail(PK_EINVAL, "pk_cost: boundary term needs h%s");
+    if (spec->w_area != 0.f && !h) return pk_fail(PK_EINVAL, "pk_cost: area term needs h%s");
+    if (spec->pair_mode == PK_PAIR_LUT) {
+        const PkLut& L = spec->lut;
+        if (!L.vals || L.nx < 2 || L.ny < 2 || L.nt < 2)
+            return pk_fail(PK_EINVAL, "pk_cost: LUT needs vals and at least 2 points per axis%s");
+    }
+    const int T = pk_cost_threads(n_max);
+    const int cap = pk_cost_cap(T, spec->pair_mode);
+    const size_t smem = pk_cost_smem_bytes(n_max, cap);
+    cudaError_t err = cudaSuccess;
+    switch (spec->pair_mode) {
+#define PK_CASE(M)                                                                                  \
+    case M:                                                                                         \
+        err = cudaFuncSetAttribute(pk_cost_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                   (int)smem);                                                      \
+        if (err == cudaSuccess) {                                                                   \
+            pk_cost_kernel<M><<<E, T, smem, st>>>(xyt, offsets, E, n_max, h, *spec, cost, grad,     \
+                                                  grad_h, cap);                                     \
+            err = cudaGetLastError();                                                               \
+        }                                                                                           \
+        break;
+        PK_CASE(PK_PAIR_NONE)
+        PK_CASE(PK_PAIR_AREA)
+        PK_CASE(PK_PAIR_SEP)
+        PK_CASE(PK_PAIR_LUT)
+#undef PK_CASE
+        default:
+            return pk_fail(PK_EINVAL, "pk_cost: unknown pair_mode%s");
+    }
+    return pk_cuda_check(err, "pk_cost launch");
+}
+
+extern "C" int pk_cost(const float* xyt, const int* offsets, int E, int n_uniform, const float* h,
+                       const PkCostSpec* spec, float* cost, float* grad, float* grad_h, void* stream)
+{
+    return pk_launch_cost(xyt, offsets, E, n_uniform, h, spec, cost, grad, grad_h, (cudaStream_t)stream);
+}
+
+extern "C" int pk_overlap(const float* xyt, int E, int n, int use_separation, float* cost, float* grad,
+                          void* stream)
+{
+    PkCostSpec s;
+    memset(&s, 0, sizeof(s));
+    s.pair_mode = use_separation ? PK_PAIR_SEP : PK_PAIR_AREA;
+    s.w_pair = 1.f;
+    return pk_launch_cost(xyt, nullptr, E, n, nullptr, &s, cost, grad, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int pk_boundary(const float* xyt, const float* h, int E, int n, float* cost, float* grad,
+                           float* grad_h, void* stream)
+{
+    PkCostSpec s;
+    memset(&s, 0, sizeof(s));
+    s.pair_mode = PK_PAIR_NONE;
+    s.w_boundary = 1.f;
+    return pk_launch_cost(xyt, nullptr, E, n, h, &s, cost, grad, grad_h, (cudaStream_t)stream);
+}
+
+extern "C" int pk_overlap_lut(const float* xyt, const int* offsets, int E, int n_uniform, const PkLut* lut,
+                              float* cost, float* grad, void* stream)
+{
+    if (!lut) return pk_fail(PK_EINVAL, "pk_overlap_lut: lut is NULL%s");
+    PkCostSpec s;
+    memset(&s, 0, sizeof(s));
+    s.pair_mode = PK_PAIR_LUT;
+    s.w_pair = 1.f;
+    s.lut = *lut;
+    return pk_launch_cost(xyt, offsets, E, n_uniform, nullptr, &s, cost, grad, nullptr, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// LUT construction from the analytic pair cost: vals[ix, iy, it] = cost of
+// a tree at the origin (theta 0) and one at (X[ix], Y[iy], T[it]) -- the
+// eval_fn of CollisionCost._ensure_lut_initialized (pack_cost.py:333-377),
+// which evaluates 2-tree ensembles with the kernel cost.  Thread per grid
+// point; all 16 piece pairs after the centre and AABB culls.
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void pk_lut_build_kernel(const float* __restrict__ X, int nx, const float* __restrict__ Y, int ny,
+                                    const float* __restrict__ Tt, int nt, float* __restrict__ vals)
+{
+    const size_t total = (size_t)nx * ny * nt;
+    for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < total; w += (size_t)gridDim.x * blockDim.x) {
+        const int it = (int)(w % nt);
+        const int iy = (int)((w / nt) % ny);
+        const int ix = (int)(w / ((size_t)nt * ny));
+        const float2 d = make_float2(X[ix], Y[iy]);
+        float acc = 0.f;
+        if (d.x * d.x + d.y * d.y <= c_geom.cutoff_sq) {
+            float s, c;
+            sincosf(Tt[it], &s, &c);
+#pragma unroll 1
+            for (int p = 0; p < 4; ++p) {
+                float2 P[4];
+                float4 bp = make_float4(1e30f, -1e30f, 1e30f, -1e30f);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    P[v] = c_geom.piece[p][v];
+                    bp.x = fminf(bp.x, P[v].x); bp.y = fmaxf(bp.y, P[v].x);
+                    bp.z = fminf(bp.z, P[v].y); bp.w = fmaxf(bp.w, P[v].y);
+                }
+#pragma unroll 1
+                for (int q = 0; q < 4; ++q) {
+                    float2 Q[4];
+                    float4 bq = make_float4(1e30f, -1e30f, 1e30f, -1e30f);
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        const float2 l = c_geom.piece[q][v];
+                        Q[v] = make_float2(c * l.x - s * l.y + d.x, s * l.x + c * l.y + d.y);
+                        bq.x = fminf(bq.x, Q[v].x); bq.y = fmaxf(bq.y, Q[v].x);
+                        bq.z = fminf(bq.z, Q[v].y); bq.w = fmaxf(bq.w, Q[v].y);
+                    }
+                    if (bp.y < bq.x || bq.y < bp.x || bp.w < bq.z || bq.w < bp.z) continue;
+                    float val;
+                    float3 gp, gq;
+                    const bool pt = c_geom.piece_nv[p] == 3, qt = c_geom.piece_nv[q] == 3;
+                    if (MODE == PK_PAIR_AREA) {
+                        pk_piece_area_grad(P, pt, Q, qt, d, val, gp, gq);
+                    } else {
+                        float sp;
+                        pk_piece_sat_grad(P, pt, Q, qt, d, sp, gp, gq);
+                        val = sp * sp;
+                    }
+                    acc += val;
+                }
+            }
+        }
+        vals[w] = acc;
+    }
+}
+
+extern "C" int pk_lut_build(const float* X, int nx, const float* Y, int ny, const float* T, int nt, int pair_mode,
+                            float* vals, void* stream)
+{
+    int rc = pk_check_init();
+    if (rc) return rc;
+    if (nx < 1 || ny < 1 || nt < 1) return pk_fail(PK_EINVAL, "pk_lut_build: empty grid%s");
+    if (!X || !Y || !T || !vals) return pk_fail(PK_EINVAL, "pk_lut_build: NULL pointer%s");
+    const size_t total = (size_t)nx * ny * nt;
+    const int blocks = (int)((total + 255) / 256 < 148 * 32 ? (total + 255) / 256 : 148 * 32);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (pair_mode == PK_PAIR_AREA)
+        pk_lut_build_kernel<PK_PAIR_AREA><<<blocks, 256, 0, st>>>(X, nx, Y, ny, T, nt, vals);
+    else if (pair_mode == PK_PAIR_SEP)
+        pk_lut_build_kernel<PK_PAIR_SEP><<<blocks, 256, 0, st>>>(X, nx, Y, ny, T, nt, vals);
+    else
+        return pk_fail(PK_EINVAL, "pk_lut_build: pair_mode must be AREA or SEP%s");
+    return pk_cuda_check(cudaGetLastError(), "pk_lut_build launch");
+}

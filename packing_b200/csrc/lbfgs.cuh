@@ -1,0 +1,485 @@
+// lbfgs.cuh -- batched L-BFGS (lbfgs_torch_parallel.py:411-729, no line search).
+//
+// Two forms share the per-system arithmetic below:
+//  * the drop-in kernels (pk_lbfgs_direction / _step / _update) run one
+//    iteration phase each for M independent systems while the objective
+//    stays a caller-supplied function (the reference's `func`);
+//  * pk_relax_kernel runs whole relaxations: one CTA per packing keeps x,
+//    the gradient and the direction in shared memory, evaluates the compound
+//    cost with the cost kernel's device code and iterates to max_iter in a
+//    single launch.
+// History is a ring buffer (logical entry i of a system lives in slot
+// (start + i) % m), which is equivalent to the reference's shift-left-and-
+// append (:676-690) without moving memory.
+#pragma once
+#include "common.cuh"
+#include "cost.cuh"
+
+template <typename F>
+__device__ __forceinline__ F pk_bsum(F v, F* red) { return pk_block_sum<F>(v, red); }
+
+template <typename F>
+__device__ __forceinline__ F pk_bmax(F v, F* red) { return pk_block_max<F>(v, red); }
+
+// Two-loop recursion (:533-572) for one system: d = -H g with the valid
+// history entries in logical order; al is shared scratch of m entries.
+template <typename F>
+__device__ void pk_two_loop(const F* g, F* d, int N, const F* S, const F* Y, const F* ro, int m, int hlen,
+                            int hstart, F Hdiag, F* al, F* red)
+{
+    for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = -g[k];
+    __syncthreads();
+    for (int i = hlen - 1; i >= 0; --i) {
+        const int slot = (hstart + i) % m;
+        const F* s = S + (size_t)slot * N;
+        const F* y = Y + (size_t)slot * N;
+        F part = 0;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) part += s[k] * d[k];
+        const F a = pk_bsum<F>(part, red) * ro[slot];
+        if (threadIdx.x == 0) al[i] = a;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = d[k] - y[k] * a;
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = d[k] * Hdiag;
+    __syncthreads();
+    for (int i = 0; i < hlen; ++i) {
+        const int slot = (hstart + i) % m;
+        const F* s = S + (size_t)slot * N;
+        const F* y = Y + (size_t)slot * N;
+        F part = 0;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) part += y[k] * d[k];
+        const F be = pk_bsum<F>(part, red) * ro[slot];
+        const F c = al[i] - be;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = d[k] + s[k] * c;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Drop-in kernels.  Per-system state (all device arrays of M entries):
+//   loss, prev_loss, loss0 (F); t, H (F); hlen, hstart, evals, active (int)
+// ---------------------------------------------------------------------------
+template <typename F>
+struct PkLbfgsState {
+    F* x; F* g; F* loss; F* d; F* pg; F* ploss; F* loss0;
+    F* S; F* Y; F* ro; F* H; F* t;
+    int* hlen; int* hstart; int* evals; int* active; int* any_active;
+    int M, N, m;
+};
+
+// Phase 1 of an iteration (:531-612): direction, initial step, max_step
+// clamp, directional-derivative stop.  Sets *any_active if a system remains.
+template <typename F>
+__global__ void pk_lbfgs_direction_kernel(PkLbfgsState<F> s, int n_iter, F lr, F max_step, int has_max_step,
+                                          F tol_change)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    F* red = (F*)pk_smem;
+    F* al = red + 32;
+    const int b = blockIdx.x;
+    const int N = s.N;
+    const F* g = s.g + (size_t)b * N;
+    F* d = s.d + (size_t)b * N;
+    F* pg = s.pg + (size_t)b * N;
+    int active = s.active[b];
+    F Hd = s.H[b];
+    if (n_iter == 1) {
+        for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = -g[k];
+        Hd = 1;
+        __syncthreads();
+    } else {
+        pk_two_loop<F>(g, d, N, s.S + (size_t)b * s.m * N, s.Y + (size_t)b * s.m * N, s.ro + (size_t)b * s.m, s.m,
+                       s.hlen[b], s.hstart[b], Hd, al, red);
+    }
+    for (int k = threadIdx.x; k < N; k += blockDim.x) pg[k] = g[k];
+    F t;
+    if (n_iter == 1) {
+        F part = 0;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) part += fabs(g[k]);
+        const F gs = pk_bsum<F>(part, red);
+        t = (F)1 / gs;
+        t = (t < (F)1 ? t : (F)1) * lr;   // torch.minimum(1, 1/sum|g|) * lr
+        if (!active) t = 0;
+    } else {
+        t = lr;
+    }
+    if (has_max_step) {
+        F part = 0;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) part = fmax(part, fabs(d[k] * t));
+        const F pc = pk_bmax<F>(part, red);
+        if (pc > max_step) t = t * (max_step / pc);
+    }
+    F part = 0;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) part += g[k] * d[k];
+    const F gtd = pk_bsum<F>(part, red);
+    if (gtd > -tol_change) active = 0;
+    if (threadIdx.x == 0) {
+        s.t[b] = t;
+        s.H[b] = Hd;
+        s.ploss[b] = s.loss[b];
+        s.active[b] = active;
+        if (active) atomicOr(s.any_active, 1);
+    }
+}
+
+// Phase 2 (:631): x += t d for every system (inactive ones too, as the
+// reference does while any system is active).
+template <typename F>
+__global__ void pk_lbfgs_step_kernel(F* x, const F* d, const F* t, int M, int N)
+{
+    const size_t total = (size_t)M * N;
+    for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < total; w += (size_t)gridDim.x * blockDim.x)
+        x[w] = x[w] + t[w / N] * d[w];
+}
+
+// Phase 3 (:636-724): history update with the curvature guard, then the
+// convergence tests.  g / loss are the values at the new x (unchanged when
+// the objective was not re-evaluated on the last iteration).
+template <typename F>
+__global__ void pk_lbfgs_update_kernel(PkLbfgsState<F> s, int n_iter, F tol_grad, F tol_change, F tol_rel,
+                                       int stop_on_increase, int max_eval)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    F* red = (F*)pk_smem;
+    const int b = blockIdx.x;
+    const int N = s.N, m = s.m;
+    const F* g = s.g + (size_t)b * N;
+    const F* pg = s.pg + (size_t)b * N;
+    const F* d = s.d + (size_t)b * N;
+    const F t = s.t[b];
+    int active = s.active[b];
+    int evals = s.evals[b] + 1;
+    if (n_iter > 1) {
+        F pys = 0, pyy = 0;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) {
+            const F y = g[k] - pg[k], sv = d[k] * t;
+            pys += y * sv;
+            pyy += y * y;
+        }
+        const F ys = pk_bsum<F>(pys, red);
+        const F yy = pk_bsum<F>(pyy, red);
+        if (active && ys > (F)1e-10) {
+            int hl = s.hlen[b], hs = s.hstart[b], slot;
+            if (hl < m) { slot = (hs + hl) % m; ++hl; }
+            else { slot = hs; hs = (hs + 1) % m; }
+            F* S = s.S + ((size_t)b * m + slot) * N;
+            F* Y = s.Y + ((size_t)b * m + slot) * N;
+            for (int k = threadIdx.x; k < N; k += blockDim.x) {
+                Y[k] = g[k] - pg[k];
+                S[k] = d[k] * t;
+            }
+            if (threadIdx.x == 0) {
+                s.H[b] = ys / yy;
+                s.ro[(size_t)b * m + slot] = (F)1 / ys;
+                s.hlen[b] = hl;
+                s.hstart[b] = hs;
+            }
+        }
+    }
+    F pmx = 0, pch = 0;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        pmx = fmax(pmx, fabs(g[k]));
+        pch = fmax(pch, fabs(d[k] * t));
+    }
+    const F gmax = pk_bmax<F>(pmx, red);
+    const F pc = pk_bmax<F>(pch, red);
+    if (threadIdx.x == 0) {
+        if (gmax <= tol_grad) active = 0;
+        if (evals >= max_eval) active = 0;
+        if (pc <= tol_change && active) active = 0;
+        const F loss = s.loss[b], ploss = s.ploss[b];
+        const F lc = fabs(loss - ploss);
+        if (lc < tol_change && active) active = 0;
+        if (tol_rel > 0 && n_iter > m) {
+            if (lc / (fabs(ploss) + (F)1e-12) < tol_rel && active) active = 0;
+        }
+        if (stop_on_increase && loss > s.loss0[b] && active) active = 0;
+        s.active[b] = active;
+        s.evals[b] = evals;
+    }
+}
+
+// Initial activity (:493-500): active unless max|g| <= tol_grad.
+template <typename F>
+__global__ void pk_lbfgs_init_kernel(PkLbfgsState<F> s, F tol_grad)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    F* red = (F*)pk_smem;
+    const int b = blockIdx.x;
+    const F* g = s.g + (size_t)b * s.N;
+    F p = 0;
+    for (int k = threadIdx.x; k < s.N; k += blockDim.x) p = fmax(p, fabs(g[k]));
+    const F gm = pk_bmax<F>(p, red);
+    if (threadIdx.x == 0) {
+        const int a = gm <= tol_grad ? 0 : 1;
+        s.active[b] = a;
+        s.hlen[b] = 0;
+        s.hstart[b] = 0;
+        s.evals[b] = 1;
+        s.H[b] = 1;
+        s.loss0[b] = s.loss[b];
+        if (a) atomicOr(s.any_active, 1);
+    }
+}
+
+static inline int pk_lbfgs_threads(int N) { return N >= 1024 ? 256 : (N >= 256 ? 128 : 64); }
+
+template <typename F>
+static int pk_lbfgs_phase(int phase, const PkLbfgsState<F>& s, int n_iter, double a, double b_, double c, double d_,
+                          int i1, int i2, cudaStream_t st)
+{
+    const int T = pk_lbfgs_threads(s.N);
+    const size_t smem = (32 + (size_t)(s.m > 0 ? s.m : 1)) * sizeof(F);
+    if (s.M == 0) return PK_OK;
+    switch (phase) {
+        case 0: pk_lbfgs_init_kernel<F><<<s.M, T, smem, st>>>(s, (F)a); break;
+        case 1: pk_lbfgs_direction_kernel<F><<<s.M, T, smem, st>>>(s, n_iter, (F)a, (F)b_, i1, (F)c); break;
+        case 2: {
+            const size_t total = (size_t)s.M * s.N;
+            const int blocks = (int)((total + 255) / 256 < 148 * 8 ? (total + 255) / 256 : 148 * 8);
+            pk_lbfgs_step_kernel<F><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(s.x, s.d, s.t, s.M, s.N);
+            break;
+        }
+        case 3: pk_lbfgs_update_kernel<F><<<s.M, T, smem, st>>>(s, n_iter, (F)a, (F)b_, (F)c, i1, i2); break;
+        default: return pk_fail(PK_EINVAL, "pk_lbfgs: unknown phase%s");
+    }
+    (void)d_;
+    return pk_cuda_check(cudaGetLastError(), "pk_lbfgs launch");
+}
+
+// C-ABI: the state struct is passed as pointers to device arrays.
+extern "C" int pk_lbfgs_phase(int phase, int dtype_bytes, void* const* arrays, int M, int N, int m, int n_iter,
+                              double p0, double p1, double p2, double p3, int i1, int i2, void* stream)
+{
+    if (!arrays) return pk_fail(PK_EINVAL, "pk_lbfgs_phase: arrays is NULL%s");
+    if (M < 0 || N < 1 || m < 1) return pk_fail(PK_EINVAL, "pk_lbfgs_phase: bad sizes%s");
+    cudaStream_t st = (cudaStream_t)stream;
+#define PK_FILL(F)                                                                                     \
+    PkLbfgsState<F> s;                                                                                 \
+    s.x = (F*)arrays[0]; s.g = (F*)arrays[1]; s.loss = (F*)arrays[2]; s.d = (F*)arrays[3];             \
+    s.pg = (F*)arrays[4]; s.ploss = (F*)arrays[5]; s.loss0 = (F*)arrays[6]; s.S = (F*)arrays[7];        \
+    s.Y = (F*)arrays[8]; s.ro = (F*)arrays[9]; s.H = (F*)arrays[10]; s.t = (F*)arrays[11];             \
+    s.hlen = (int*)arrays[12]; s.hstart = (int*)arrays[13]; s.evals = (int*)arrays[14];                \
+    s.active = (int*)arrays[15]; s.any_active = (int*)arrays[16];                                      \
+    s.M = M; s.N = N; s.m = m;
+    if (dtype_bytes == 4) {
+        PK_FILL(float)
+        return pk_lbfgs_phase<float>(phase, s, n_iter, p0, p1, p2, p3, i1, i2, st);
+    } else if (dtype_bytes == 8) {
+        PK_FILL(double)
+        return pk_lbfgs_phase<double>(phase, s, n_iter, p0, p1, p2, p3, i1, i2, st);
+    }
+#undef PK_FILL
+    return pk_fail(PK_EINVAL, "pk_lbfgs_phase: dtype must be float32 or float64%s");
+}
+
+// ---------------------------------------------------------------------------
+// Fused relaxation: one CTA per packing runs the whole L-BFGS loop with the
+// compound cost evaluated in place.  x = [xyt (3n), h (3)] as in
+// pack_dynamics.py:76-83.  Per-instance stop: an instance that becomes
+// inactive stops stepping (the reference keeps stepping inactive systems
+// while another system of the same batch is still active, so with this form
+// an instance's result never depends on the rest of the batch).
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void pk_relax_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in,
+                                const int* __restrict__ offsets, const int* __restrict__ order, int E, int n_max,
+                                PkCostSpec spec, PkRelaxParams prm, float* __restrict__ xyt_out,
+                                float* __restrict__ h_out, float* __restrict__ loss_out, int* __restrict__ iters_out,
+                                float* __restrict__ work, int cap)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    const int e = order ? order[blockIdx.x] : blockIdx.x;
+    if (e < 0 || e >= E) return;
+    const int base = offsets ? offsets[e] : e * n_max;
+    const int n = offsets ? offsets[e + 1] - base : n_max;
+    if (n < 0 || n > n_max) {
+        if (threadIdx.x == 0) { loss_out[e] = __int_as_float(0x7fc00000); if (iters_out) iters_out[e] = -1; }
+        return;
+    }
+    const int N = 3 * n + 3;
+    const int NM = 3 * n_max + 3;
+    const int m = prm.history;
+    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap);
+    if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
+    float* x = (float*)(pk_smem + pk_cost_smem_bytes(n_max, cap));
+    float* g = x + NM;
+    float* pg = g + NM;
+    float* d = pg + NM;
+    float* al = d + NM;
+    float* ro = al + m;
+    float* red = ro + m;
+    // history of this instance: work + 2 m * (3 * base + 3 * e) floats
+    float* S = work + (size_t)2 * m * (3 * (size_t)base + 3 * (size_t)e);
+    float* Y = S + (size_t)m * N;
+    for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) x[k] = xyt_in[(size_t)base * 3 + k];
+    if (threadIdx.x < 3) x[3 * n + threadIdx.x] = h_in ? h_in[3 * e + threadIdx.x] : 0.f;
+    __syncthreads();
+    const bool use_h = h_in != nullptr;
+    double L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, g, use_h ? g + 3 * n : nullptr, sm);
+    if (!use_h && threadIdx.x < 3) g[3 * n + threadIdx.x] = 0.f;
+    __syncthreads();
+    float loss = (float)L;
+    const float loss0 = loss;
+    float gm = 0.f;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) gm = fmaxf(gm, fabsf(g[k]));
+    gm = pk_bmax<float>(gm, red);
+    bool active = !(gm <= prm.tol_grad);
+    int evals = 1, hlen = 0, hstart = 0, it = 0;
+    unsigned long long hist_streamed = 0;
+    float H = 1.f;
+    while (active && it < prm.max_iter) {
+        ++it;
+        if (it == 1) {
+            for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = -g[k];
+            H = 1.f;
+            __syncthreads();
+        } else {
+            pk_two_loop<float>(g, d, N, S, Y, ro, m, hlen, hstart, H, al, red);
+            hist_streamed += (unsigned long long)hlen;
+        }
+        for (int k = threadIdx.x; k < N; k += blockDim.x) pg[k] = g[k];
+        const float ploss = loss;
+        float t;
+        if (it == 1) {
+            float p = 0.f;
+            for (int k = threadIdx.x; k < N; k += blockDim.x) p += fabsf(g[k]);
+            const float gs = pk_bsum<float>(p, red);
+            t = 1.f / gs;
+            t = (t < 1.f ? t : 1.f) * prm.lr;
+        } else {
+            t = prm.lr;
+        }
+        if (prm.has_max_step) {
+            float p = 0.f;
+            for (int k = threadIdx.x; k < N; k += blockDim.x) p = fmaxf(p, fabsf(d[k] * t));
+            const float pc = pk_bmax<float>(p, red);
+            if (pc > prm.max_step) t = t * (prm.max_step / pc);
+        }
+        {
+            float p = 0.f;
+            for (int k = threadIdx.x; k < N; k += blockDim.x) p += g[k] * d[k];
+            const float gtd = pk_bsum<float>(p, red);
+            if (gtd > -prm.tol_change) { active = false; --it; break; }
+        }
+        for (int k = threadIdx.x; k < N; k += blockDim.x) x[k] = x[k] + t * d[k];
+        __syncthreads();
+        if (it != prm.max_iter) {
+            L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, g, use_h ? g + 3 * n : nullptr, sm);
+            loss = (float)L;
+            if (!use_h && threadIdx.x < 3) g[3 * n + threadIdx.x] = 0.f;
+            __syncthreads();
+        }
+        ++evals;
+        if (it > 1) {
+            float pys = 0.f, pyy = 0.f;
+            for (int k = threadIdx.x; k < N; k += blockDim.x) {
+                const float y = g[k] - pg[k], sv = d[k] * t;
+                pys += y * sv;
+                pyy += y * y;
+            }
+            const float ys = pk_bsum<float>(pys, red);
+            const float yy = pk_bsum<float>(pyy, red);
+            if (ys > 1e-10f) {
+                int slot;
+                if (hlen < m) { slot = (hstart + hlen) % m; ++hlen; }
+                else { slot = hstart; hstart = (hstart + 1) % m; }
+                float* Sd = S + (size_t)slot * N;
+                float* Yd = Y + (size_t)slot * N;
+                for (int k = threadIdx.x; k < N; k += blockDim.x) {
+                    Yd[k] = g[k] - pg[k];
+                    Sd[k] = d[k] * t;
+                }
+                H = ys / yy;
+                if (threadIdx.x == 0) ro[slot] = 1.f / ys;
+                __syncthreads();
+            }
+        }
+        float pmx = 0.f, pch = 0.f;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) {
+            pmx = fmaxf(pmx, fabsf(g[k]));
+            pch = fmaxf(pch, fabsf(d[k] * t));
+        }
+        const float gmax = pk_bmax<float>(pmx, red);
+        const float pc = pk_bmax<float>(pch, red);
+        if (gmax <= prm.tol_grad) active = false;
+        if (evals >= prm.max_eval) active = false;
+        if (pc <= prm.tol_change) active = false;
+        const float lc = fabsf(loss - ploss);
+        if (lc < prm.tol_change) active = false;
+        if (prm.tol_rel_change > 0.f && it > m && lc / (fabsf(ploss) + 1e-12f) < prm.tol_rel_change) active = false;
+        if (prm.stop_on_cost_increase && loss > loss0) active = false;
+    }
+    if (prm.final_eval) {
+        L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, nullptr, nullptr, sm);
+        loss = (float)L;
+    }
+    for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) xyt_out[(size_t)base * 3 + k] = x[k];
+    if (h_out && threadIdx.x < 3) h_out[3 * e + threadIdx.x] = x[3 * n + threadIdx.x];
+    if (threadIdx.x == 0) {
+        loss_out[e] = loss;
+        if (iters_out) iters_out[e] = it;
+        if (prm.counters) {
+            for (int k = 0; k < 4; ++k) atomicAdd(&prm.counters[k], (unsigned long long)sm.cnt[k]);
+            atomicAdd(&prm.counters[4], (unsigned long long)it);
+            atomicAdd(&prm.counters[5], hist_streamed * (unsigned long long)N);
+        }
+    }
+}
+
+static size_t pk_relax_smem_bytes(int n_max, int cap, int m)
+{
+    const int NM = 3 * n_max + 3;
+    return pk_cost_smem_bytes(n_max, cap) + ((size_t)4 * NM + 2 * (size_t)m + 64) * 4;
+}
+
+extern "C" size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, int history)
+{
+    size_t tot = 0;
+    if (sizes_host) {
+        for (int e = 0; e < E; ++e) tot += 3 * (size_t)sizes_host[e] + 3;
+    } else {
+        tot = (size_t)E * (3 * (size_t)n_uniform + 3);
+    }
+    return 2 * (size_t)history * tot;
+}
+
+extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offsets, const int* order, int E,
+                        int n_max, const PkCostSpec* spec, const PkRelaxParams* prm, float* xyt_out, float* h_out,
+                        float* loss_out, int* iters_out, float* work, void* stream)
+{
+    int rc = pk_check_init();
+    if (rc) return rc;
+    if (!spec || !prm) return pk_fail(PK_EINVAL, "pk_relax: spec and params are required%s");
+    if (E < 0 || n_max < 0) return pk_fail(PK_EINVAL, "pk_relax: negative size%s");
+    if (E == 0) return PK_OK;
+    if (n_max > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_relax: more than 1024 trees per instance%s");
+    if (prm->history < 1 || prm->history > 64) return pk_fail(PK_EINVAL, "pk_relax: history must be in [1, 64]%s");
+    if (!xyt_in || !xyt_out || !loss_out || !work) return pk_fail(PK_EINVAL, "pk_relax: NULL pointer%s");
+    if ((spec->w_boundary != 0.f || spec->w_area != 0.f) && !h_in)
+        return pk_fail(PK_EINVAL, "pk_relax: boundary / area terms need h%s");
+    if (spec->pair_mode == PK_PAIR_LUT && !spec->lut.vals) return pk_fail(PK_EINVAL, "pk_relax: LUT without vals%s");
+    const int T = pk_cost_threads(n_max);
+    // the item list must hold one full round (16 piece pairs per thread) beyond its flush level
+    const int cap = spec->pair_mode == PK_PAIR_LUT ? 4 * T : 20 * T;
+    const size_t smem = pk_relax_smem_bytes(n_max, cap, prm->history);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t err = cudaSuccess;
+    switch (spec->pair_mode) {
+#define PK_R(M)                                                                                          \
+    case M:                                                                                              \
+        err = cudaFuncSetAttribute(pk_relax_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        if (err == cudaSuccess)                                                                          \
+            pk_relax_kernel<M><<<E, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, xyt_out, \
+                                                   h_out, loss_out, iters_out, work, cap);                \
+        break;
+        PK_R(PK_PAIR_NONE)
+        PK_R(PK_PAIR_AREA)
+        PK_R(PK_PAIR_SEP)
+        PK_R(PK_PAIR_LUT)
+#undef PK_R
+        default: return pk_fail(PK_EINVAL, "pk_relax: unknown pair_mode%s");
+    }
+    if (err != cudaSuccess) return pk_cuda_check(err, "pk_relax attribute");
+    return pk_cuda_check(cudaGetLastError(), "pk_relax launch");
+}

@@ -1,0 +1,130 @@
+"""Batched L-BFGS: the CUDA drop-in against the oracle restatement (itself
+pinned to the reference's lbfgs), and the fused relaxation against the
+drop-in driving the same cost kernel."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.workloads import poses, square_h
+
+pytestmark = pytest.mark.gpu
+
+
+def _quad_problem(M=6, N=40, seed=0):
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(M, N, N))
+    A = A @ A.transpose(0, 2, 1) / N + np.eye(N)[None]
+    b = rng.normal(size=(M, N))
+    x0 = rng.normal(size=(M, N)) * 2
+    return A, b, x0
+
+
+@pytest.mark.parametrize("kw", [
+    dict(max_iter=30, history_size=5, max_step=0.5, tolerance_grad=0, tolerance_change=0),
+    dict(max_iter=40, history_size=3, max_step=0.2, tolerance_grad=1e-6, tolerance_change=1e-9),
+    dict(max_iter=25, history_size=30, max_step=None, tolerance_grad=0, tolerance_change=0, lr=0.7),
+    dict(max_iter=30, history_size=4, max_step=1.0, stop_on_cost_increase=True, tolerance_rel_change=1e-3),
+])
+def test_dropin_fp64_matches_oracle(cuda, kw):
+    from packing_b200.lbfgs_torch_parallel import lbfgs
+    A, b, x0 = _quad_problem()
+    At, bt = torch.from_numpy(A).to(cuda), torch.from_numpy(b).to(cuda)
+
+    def f(x, is_main):
+        Ax = torch.einsum("mij,mj->mi", At, x)
+        return 0.5 * (x * Ax).sum(1) - (bt * x).sum(1), Ax - bt
+
+    def fo(x):
+        Ax = np.einsum("mij,mj->mi", A, x)
+        return 0.5 * (x * Ax).sum(1) - (b * x).sum(1), Ax - b
+
+    x = torch.from_numpy(x0.copy()).to(cuda)
+    out = lbfgs(f, x, **kw)
+    assert out is x
+    xo, _ = O.lbfgs(fo, x0, **kw)
+    np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=0, atol=1e-9)
+
+
+def _pack_func(n, E, dev):
+    from packing_b200.cost import CostSpec, compound_cost
+    spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
+
+    def f(x, is_main):
+        xyt = x[:, :3 * n].reshape(E, n, 3).contiguous()
+        h = x[:, 3 * n:].contiguous()
+        c, g, gh = compound_cost(xyt, h, spec)
+        return c, torch.cat([g.reshape(E, -1), gh], 1)
+    return f, spec
+
+
+def test_dropin_fp32_packing_matches_oracle(cuda):
+    """Short FP32 relaxation (kernel cost) vs the FP64 oracle relaxation."""
+    from packing_b200.lbfgs_torch_parallel import lbfgs
+    n, E = 12, 5
+    xyt = poses(E, n, seed=21)
+    h = square_h(E, n)
+    x0 = np.concatenate([xyt.reshape(E, -1), h], 1)
+    f, _ = _pack_func(n, E, cuda)
+    x = torch.from_numpy(x0.astype(np.float32)).to(cuda)
+    lbfgs(f, x, max_iter=8, history_size=3, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+
+    def fo(xx):
+        c, g, gh = O.compound_cost(xx[:, :3 * n].reshape(E, n, 3), xx[:, 3 * n:], w_area=1e-2, fixed_h=True)
+        return c, np.concatenate([g.reshape(E, -1), gh], 1)
+
+    xo, _ = O.lbfgs(fo, x0.astype(np.float64), max_iter=8, history_size=3, max_step=0.01, tolerance_grad=0,
+                    tolerance_change=0)
+    np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=0, atol=2e-4)
+
+
+def test_fused_relax_matches_dropin(cuda):
+    """The one-launch relaxation and the drop-in lbfgs over the same kernel
+    cost follow the same iterates (FP32, reduction order aside)."""
+    from packing_b200.lbfgs_torch_parallel import lbfgs
+    from packing_b200.relax import RelaxParams, relax
+    n, E = 30, 8
+    xyt = poses(E, n, seed=31)
+    h = square_h(E, n)
+    f, spec = _pack_func(n, E, cuda)
+    for iters, hist in [(6, 3), (20, 10)]:
+        x = torch.from_numpy(np.concatenate([xyt.reshape(E, -1), h], 1)).to(cuda)
+        lbfgs(f, x, max_iter=iters, history_size=hist, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+        prm = RelaxParams(n_iterations=iters, history_size=hist, max_step=0.01, final_eval=True)
+        xr, hr, loss, it = relax(torch.from_numpy(xyt).to(cuda), torch.from_numpy(h).to(cuda), spec, prm)
+        assert torch.all(it == iters)
+        np.testing.assert_allclose(xr.reshape(E, -1).cpu().numpy(), x[:, :3 * n].cpu().numpy(), rtol=0,
+                                   atol=5e-5 if iters < 10 else 5e-4)
+        assert torch.equal(hr, torch.from_numpy(h).to(cuda))
+        c, _ = f(x, True)
+        np.testing.assert_allclose(loss.cpu().numpy(), c.cpu().numpy(), rtol=1e-3, atol=1e-5)
+
+
+def test_fused_relax_alone_equals_in_mix(cuda):
+    """An instance relaxed alone and inside a ragged batch gives the same bits."""
+    from packing_b200.cost import CostSpec
+    from packing_b200.relax import RelaxParams, relax_ragged
+    spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
+    prm = RelaxParams(n_iterations=40, history_size=5, max_step=0.01)
+    sizes = [10, 57, 200, 33]
+    xs = [torch.from_numpy(poses(1, s, seed=40 + s)[0]).to(cuda) for s in sizes]
+    hs = torch.from_numpy(np.concatenate([square_h(1, s) for s in sizes])).to(cuda)
+    outs, ho, loss, it = relax_ragged(xs, hs, spec, prm)
+    for e, s in enumerate(sizes):
+        o1, h1, l1, i1 = relax_ragged([xs[e]], hs[e:e + 1], spec, prm)
+        assert torch.equal(o1[0], outs[e])
+        assert torch.equal(l1, loss[e:e + 1])
+    assert float(loss.max()) < float("inf")
+
+
+def test_relaxation_reduces_cost(cuda):
+    from packing_b200.cost import CostSpec, compound_cost
+    from packing_b200.relax import RelaxParams, relax
+    spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
+    xyt = torch.from_numpy(poses(16, 200, seed=7)).to(cuda)
+    h = torch.from_numpy(square_h(16, 200)).to(cuda)
+    c0, _, _ = compound_cost(xyt, h, spec, evaluate_gradient=False)
+    xr, hr, loss, it = relax(xyt, h, spec, RelaxParams(n_iterations=100, history_size=10, max_step=0.01))
+    c1, _, _ = compound_cost(xr, hr, spec, evaluate_gradient=False)
+    assert torch.allclose(c1, loss, rtol=1e-6)
+    assert torch.all(c1 < 0.5 * c0)
