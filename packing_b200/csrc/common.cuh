@@ -109,6 +109,40 @@ __device__ __forceinline__ T pk_block_max(T v, T* scratch)
     return r;
 }
 
+// Sum of get(k), k in [0, N), in an order fixed by N alone (independent of
+// blockDim): element k belongs to group k / 256 and lane k % 32; each group's
+// per-lane partial is a sequential sum in k order, warp 0 then adds the
+// groups in order per lane and finishes with a fixed shuffle tree.  red must
+// hold 32 * ceil(N / 256) entries.  Called by all threads; all get the sum.
+#define PK_CANON_GROUP 256
+template <typename T, typename Get>
+__device__ __forceinline__ T pk_canon_sum(int N, Get get, T* red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    const int ng = (N + PK_CANON_GROUP - 1) / PK_CANON_GROUP;
+    for (int grp = warp; grp < ng; grp += nw) {
+        T s = T(0);
+        const int end = min(N, (grp + 1) * PK_CANON_GROUP);
+        for (int k = grp * PK_CANON_GROUP + lane; k < end; k += 32) s += get(k);
+        red[grp * 32 + lane] = s;
+    }
+    __syncthreads();
+    T r = T(0);
+    if (warp == 0) {
+        for (int grp = 0; grp < ng; ++grp) r += red[grp * 32 + lane];
+        r = pk_warp_sum(r);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) red[0] = r;
+    __syncthreads();
+    r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__host__ __device__ inline int pk_canon_red_len(int N) { return 32 * ((N + PK_CANON_GROUP - 1) / PK_CANON_GROUP + 1); }
+
 // Bounded wrap of an angle difference into [-pi, pi], following the
 // reference's subtract-2pi loop (pack_cuda_lut.py:289-293) in FP32.  Angles
 // beyond +-64 pi are reduced with remainderf first so the loop stays short.

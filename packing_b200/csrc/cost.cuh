@@ -84,16 +84,26 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
 // P edge line is kept only if both run the same way, so a shared boundary
 // segment is counted once and touching pieces contribute zero.
 // ---------------------------------------------------------------------------
+// Near-collinear edges (all four endpoints within PK_COLLINEAR_TOL of the
+// other edge's line) are classified from the same four numbers on both
+// sides, so the P-side and Q-side decisions can never disagree.
+#define PK_COLLINEAR_TOL2 4e-12f   // (2e-6)^2, squared distance in tree units
 __device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_tri,
                                                    const float2 (&Q)[4], bool q_tri, float2 d,
                                                    float& area, float3& gP, float3& gQ)
 {
     float fPQ[4][4];   // [Q line k][P vertex v]
     float fQP[4][4];   // [P line k][Q vertex v]
+    float tP[4], tQ[4];
+    float2 eP[4], eQ[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float2 qa = Q[k], qb = Q[(k + 1) & 3];
         const float2 pa = P[k], pb = P[(k + 1) & 3];
+        eP[k] = make_float2(pb.x - pa.x, pb.y - pa.y);
+        eQ[k] = make_float2(qb.x - qa.x, qb.y - qa.y);
+        tP[k] = PK_COLLINEAR_TOL2 * (eP[k].x * eP[k].x + eP[k].y * eP[k].y);
+        tQ[k] = PK_COLLINEAR_TOL2 * (eQ[k].x * eQ[k].x + eQ[k].y * eQ[k].y);
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             fPQ[k][v] = pk_cross3(qa, qb, P[v]);
@@ -114,12 +124,15 @@ __device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_
         for (int k = 0; k < 4; ++k) {
             if (k == 3 && q_tri) continue;
             const float fa = fPQ[k][v], fb = fPQ[k][(v + 1) & 3];
+            const float ra = fQP[v][k], rb = fQP[v][(k + 1) & 3];
+            if (fa * fa <= tQ[k] && fb * fb <= tQ[k] && ra * ra <= tP[v] && rb * rb <= tP[v]) {
+                empty = true;   // collinear: the Q edge carries this boundary
+                continue;
+            }
             const bool ia = fa >= 0.f, ib = fb >= 0.f;
             if (!ia && !ib) {
                 empty = true;
-            } else if (ia && ib) {
-                if (fa == 0.f && fb == 0.f) empty = true;
-            } else {
+            } else if (ia != ib) {
                 const float t = fa / (fa - fb);
                 if (ia) tout = fminf(tout, t);
                 else tin = fmaxf(tin, t);
@@ -127,7 +140,7 @@ __device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_
         }
         if (!empty && tin < tout) {
             const float dt = tout - tin;
-            const float2 e = make_float2(b.x - a.x, b.y - a.y);
+            const float2 e = eP[v];
             A2 += dt * pk_cross(a, b);
             const float2 N = make_float2(dt * e.y, -dt * e.x);
             const float tm = 0.5f * (tin + tout);
@@ -142,22 +155,23 @@ __device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_
     for (int v = 0; v < 4; ++v) {
         if (v == 3 && q_tri) continue;
         const float2 a = Q[v], b = Q[(v + 1) & 3];
-        const float2 e = make_float2(b.x - a.x, b.y - a.y);
+        const float2 e = eQ[v];
         float tin = 0.f, tout = 1.f;
         bool empty = false;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (k == 3 && p_tri) continue;
             const float fa = fQP[k][v], fb = fQP[k][(v + 1) & 3];
+            const float ra = fPQ[v][k], rb = fPQ[v][(k + 1) & 3];
+            if (fa * fa <= tP[k] && fb * fb <= tP[k] && ra * ra <= tQ[v] && rb * rb <= tQ[v]) {
+                // collinear: kept (no constraint) when both run the same way
+                if (eP[k].x * e.x + eP[k].y * e.y <= 0.f) empty = true;
+                continue;
+            }
             const bool ia = fa >= 0.f, ib = fb >= 0.f;
             if (!ia && !ib) {
                 empty = true;
-            } else if (ia && ib) {
-                if (fa == 0.f && fb == 0.f) {
-                    const float2 pe = make_float2(P[(k + 1) & 3].x - P[k].x, P[(k + 1) & 3].y - P[k].y);
-                    if (pe.x * e.x + pe.y * e.y <= 0.f) empty = true;
-                }
-            } else {
+            } else if (ia != ib) {
                 const float t = fa / (fa - fb);
                 if (ia) tout = fminf(tout, t);
                 else tin = fmaxf(tin, t);
@@ -426,6 +440,10 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
     const bool do_bnd = spec.w_boundary != 0.f && H != nullptr;
     float half = 0.f, hox = 0.f, hoy = 0.f;
     if (H) { half = H[0] * 0.5f; hox = H[1]; hoy = H[2]; }
+    // piece table into shared memory first: phase 0 reads it
+    if (threadIdx.x < 16) sm.piece[threadIdx.x] = c_geom.piece[threadIdx.x >> 2][threadIdx.x & 3];
+    if (threadIdx.x < 4) sm.piece_nv[threadIdx.x] = c_geom.piece_nv[threadIdx.x];
+    __syncthreads();
     // ---- phase 0: per tree -------------------------------------------------
     for (int t = threadIdx.x; t < n; t += T) {
         const float x = X[3 * t], y = X[3 * t + 1], th = X[3 * t + 2];
@@ -484,8 +502,6 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
         sm.acc[3 * t + 2] = a2;
         sm.bnd[t] = bnd;
     }
-    if (threadIdx.x < 16) sm.piece[threadIdx.x] = c_geom.piece[threadIdx.x >> 2][threadIdx.x & 3];
-    if (threadIdx.x < 4) sm.piece_nv[threadIdx.x] = c_geom.piece_nv[threadIdx.x];
     if (threadIdx.x == 0) {
         *sm.count = 0;
         sm.cnt[3] += 1;
@@ -555,6 +571,7 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
             }
             __syncthreads();
             const int count = *sm.count;
+            __syncthreads();   // every thread has read count before the next round appends
             if (count > sm.cap - per_round || base + T >= npairs) {
                 pair_tot += pk_process_items<MODE>(sm, count, spec.w_pair, spec.lut);
                 __syncthreads();
@@ -646,7 +663,7 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
     if (E < 0 || n_max < 0) return pk_fail(PK_EINVAL, "pk_cost: negative size%s");
     if (E == 0) return PK_OK;
     if (n_max > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_cost: more than 1024 trees per instance%s");
-    if (!xyt || !cost) return pk_fail(PK_EINVAL, "pk_cost: xyt and cost are required%s");
+    if (!cost || (!xyt && n_max > 0)) return pk_fail(PK_EINVAL, "pk_cost: xyt and cost are required%s");
     if (spec->w_boundary != 0.f && !h) return pk_fail(PK_EINVAL, "pk_cost: boundary term needs h%s");
     if (spec->w_area != 0.f && !h) return pk_fail(PK_EINVAL, "pk_cost: area term needs h%s");
     if (spec->pair_mode == PK_PAIR_LUT) {

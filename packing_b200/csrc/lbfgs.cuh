@@ -33,9 +33,7 @@ __device__ void pk_two_loop(const F* g, F* d, int N, const F* S, const F* Y, con
         const int slot = (hstart + i) % m;
         const F* s = S + (size_t)slot * N;
         const F* y = Y + (size_t)slot * N;
-        F part = 0;
-        for (int k = threadIdx.x; k < N; k += blockDim.x) part += s[k] * d[k];
-        const F a = pk_bsum<F>(part, red) * ro[slot];
+        const F a = pk_canon_sum<F>(N, [&](int k) { return s[k] * d[k]; }, red) * ro[slot];
         if (threadIdx.x == 0) al[i] = a;
         for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = d[k] - y[k] * a;
         __syncthreads();
@@ -46,9 +44,7 @@ __device__ void pk_two_loop(const F* g, F* d, int N, const F* S, const F* Y, con
         const int slot = (hstart + i) % m;
         const F* s = S + (size_t)slot * N;
         const F* y = Y + (size_t)slot * N;
-        F part = 0;
-        for (int k = threadIdx.x; k < N; k += blockDim.x) part += y[k] * d[k];
-        const F be = pk_bsum<F>(part, red) * ro[slot];
+        const F be = pk_canon_sum<F>(N, [&](int k) { return y[k] * d[k]; }, red) * ro[slot];
         const F c = al[i] - be;
         for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = d[k] + s[k] * c;
         __syncthreads();
@@ -74,10 +70,10 @@ __global__ void pk_lbfgs_direction_kernel(PkLbfgsState<F> s, int n_iter, F lr, F
                                           F tol_change)
 {
     extern __shared__ __align__(16) unsigned char pk_smem[];
-    F* red = (F*)pk_smem;
-    F* al = red + 32;
-    const int b = blockIdx.x;
     const int N = s.N;
+    F* al = (F*)pk_smem;
+    F* red = al + s.m;
+    const int b = blockIdx.x;
     const F* g = s.g + (size_t)b * N;
     F* d = s.d + (size_t)b * N;
     F* pg = s.pg + (size_t)b * N;
@@ -94,9 +90,7 @@ __global__ void pk_lbfgs_direction_kernel(PkLbfgsState<F> s, int n_iter, F lr, F
     for (int k = threadIdx.x; k < N; k += blockDim.x) pg[k] = g[k];
     F t;
     if (n_iter == 1) {
-        F part = 0;
-        for (int k = threadIdx.x; k < N; k += blockDim.x) part += fabs(g[k]);
-        const F gs = pk_bsum<F>(part, red);
+        const F gs = pk_canon_sum<F>(N, [&](int k) { return (F)fabs(g[k]); }, red);
         t = (F)1 / gs;
         t = (t < (F)1 ? t : (F)1) * lr;   // torch.minimum(1, 1/sum|g|) * lr
         if (!active) t = 0;
@@ -109,9 +103,7 @@ __global__ void pk_lbfgs_direction_kernel(PkLbfgsState<F> s, int n_iter, F lr, F
         const F pc = pk_bmax<F>(part, red);
         if (pc > max_step) t = t * (max_step / pc);
     }
-    F part = 0;
-    for (int k = threadIdx.x; k < N; k += blockDim.x) part += g[k] * d[k];
-    const F gtd = pk_bsum<F>(part, red);
+    const F gtd = pk_canon_sum<F>(N, [&](int k) { return g[k] * d[k]; }, red);
     if (gtd > -tol_change) active = 0;
     if (threadIdx.x == 0) {
         s.t[b] = t;
@@ -150,14 +142,8 @@ __global__ void pk_lbfgs_update_kernel(PkLbfgsState<F> s, int n_iter, F tol_grad
     int active = s.active[b];
     int evals = s.evals[b] + 1;
     if (n_iter > 1) {
-        F pys = 0, pyy = 0;
-        for (int k = threadIdx.x; k < N; k += blockDim.x) {
-            const F y = g[k] - pg[k], sv = d[k] * t;
-            pys += y * sv;
-            pyy += y * y;
-        }
-        const F ys = pk_bsum<F>(pys, red);
-        const F yy = pk_bsum<F>(pyy, red);
+        const F ys = pk_canon_sum<F>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red);
+        const F yy = pk_canon_sum<F>(N, [&](int k) { const F y = g[k] - pg[k]; return y * y; }, red);
         if (active && ys > (F)1e-10) {
             int hl = s.hlen[b], hs = s.hstart[b], slot;
             if (hl < m) { slot = (hs + hl) % m; ++hl; }
@@ -229,7 +215,7 @@ static int pk_lbfgs_phase(int phase, const PkLbfgsState<F>& s, int n_iter, doubl
                           int i1, int i2, cudaStream_t st)
 {
     const int T = pk_lbfgs_threads(s.N);
-    const size_t smem = (32 + (size_t)(s.m > 0 ? s.m : 1)) * sizeof(F);
+    const size_t smem = ((size_t)s.m + pk_canon_red_len(s.N)) * sizeof(F);
     if (s.M == 0) return PK_OK;
     switch (phase) {
         case 0: pk_lbfgs_init_kernel<F><<<s.M, T, smem, st>>>(s, (F)a); break;
@@ -342,9 +328,7 @@ __global__ void pk_relax_kernel(const float* __restrict__ xyt_in, const float* _
         const float ploss = loss;
         float t;
         if (it == 1) {
-            float p = 0.f;
-            for (int k = threadIdx.x; k < N; k += blockDim.x) p += fabsf(g[k]);
-            const float gs = pk_bsum<float>(p, red);
+            const float gs = pk_canon_sum<float>(N, [&](int k) { return fabsf(g[k]); }, red);
             t = 1.f / gs;
             t = (t < 1.f ? t : 1.f) * prm.lr;
         } else {
@@ -357,9 +341,7 @@ __global__ void pk_relax_kernel(const float* __restrict__ xyt_in, const float* _
             if (pc > prm.max_step) t = t * (prm.max_step / pc);
         }
         {
-            float p = 0.f;
-            for (int k = threadIdx.x; k < N; k += blockDim.x) p += g[k] * d[k];
-            const float gtd = pk_bsum<float>(p, red);
+            const float gtd = pk_canon_sum<float>(N, [&](int k) { return g[k] * d[k]; }, red);
             if (gtd > -prm.tol_change) { active = false; --it; break; }
         }
         for (int k = threadIdx.x; k < N; k += blockDim.x) x[k] = x[k] + t * d[k];
@@ -372,14 +354,8 @@ __global__ void pk_relax_kernel(const float* __restrict__ xyt_in, const float* _
         }
         ++evals;
         if (it > 1) {
-            float pys = 0.f, pyy = 0.f;
-            for (int k = threadIdx.x; k < N; k += blockDim.x) {
-                const float y = g[k] - pg[k], sv = d[k] * t;
-                pys += y * sv;
-                pyy += y * y;
-            }
-            const float ys = pk_bsum<float>(pys, red);
-            const float yy = pk_bsum<float>(pyy, red);
+            const float ys = pk_canon_sum<float>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red);
+            const float yy = pk_canon_sum<float>(N, [&](int k) { const float y = g[k] - pg[k]; return y * y; }, red);
             if (ys > 1e-10f) {
                 int slot;
                 if (hlen < m) { slot = (hstart + hlen) % m; ++hlen; }
@@ -430,7 +406,7 @@ __global__ void pk_relax_kernel(const float* __restrict__ xyt_in, const float* _
 static size_t pk_relax_smem_bytes(int n_max, int cap, int m)
 {
     const int NM = 3 * n_max + 3;
-    return pk_cost_smem_bytes(n_max, cap) + ((size_t)4 * NM + 2 * (size_t)m + 64) * 4;
+    return pk_cost_smem_bytes(n_max, cap) + ((size_t)4 * NM + 2 * (size_t)m + pk_canon_red_len(NM)) * 4;
 }
 
 extern "C" size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, int history)

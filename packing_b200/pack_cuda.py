@@ -43,9 +43,10 @@ def overlap_multi_ensemble(xyt1, xyt2, use_separation, out_cost=None, out_grads=
     x2 = _lib.as_tensor(xyt2, "xyt2")
     if x1.ndim != 3 or x1.shape[2] != 3:
         raise ValueError(f"xyt1 must be shape (n_ensembles, n_trees, 3), got {tuple(x1.shape)}")
+    _lib.check_f32(x1, "xyt1")
+    _lib.check_f32(x2, "xyt2")
     if not _same_array(x1, x2):
         raise NotImplementedError("xyt1 and xyt2 must be the same array (every caller passes one array)")
-    _lib.check_f32(x1, "xyt1")
     E, n = int(x1.shape[0]), int(x1.shape[1])
     if out_cost is None:
         raise ValueError("out_cost must be provided")
