@@ -269,8 +269,8 @@ def run_ours(args, rank, world, dev):
         cbuf = torch.empty(Ep, device=dev)
 
         def f(x, is_main):
-            compound_cost(x[:, :3 * n].reshape(Ep, n, 3), x[:, 3 * n:], spec, out_cost=cbuf, out_grad=gbuf,
-                          out_grad_h=ghbuf)
+            compound_cost(x[:, :3 * n].reshape(Ep, n, 3).contiguous(), x[:, 3 * n:].contiguous(), spec,
+                          out_cost=cbuf, out_grad=gbuf, out_grad_h=ghbuf)
             return cbuf, torch.cat([gbuf.reshape(Ep, -1), ghbuf], 1)
 
         x0 = torch.cat([xyt[:Ep].reshape(Ep, -1), h[:Ep]], 1).contiguous()

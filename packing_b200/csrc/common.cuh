@@ -23,6 +23,7 @@ struct PkDevGeom {
     int n_tree;
     float max_radius;
     float cutoff_sq;    // (2 R)^2: farther centres cannot overlap
+    float coll_tiny;    // 2e-6 * longest piece edge: bound on |cross| of near-collinear points
 };
 
 // FP64 copy for the legality validator.
@@ -109,39 +110,43 @@ __device__ __forceinline__ T pk_block_max(T v, T* scratch)
     return r;
 }
 
-// Sum of get(k), k in [0, N), in an order fixed by N alone (independent of
-// blockDim): element k belongs to group k / 256 and lane k % 32; each group's
-// per-lane partial is a sequential sum in k order, warp 0 then adds the
-// groups in order per lane and finishes with a fixed shuffle tree.  red must
-// hold 32 * ceil(N / 256) entries.  Called by all threads; all get the sum.
+// Order-fixed vector reductions.  Element k belongs to group k / 256 and
+// lane k % 32; thread (warp w, lane l) OWNS the elements of the groups
+// g = w, w + nwarps, ... with lane l, and PK_OWN_LOOP visits exactly those.
+// Vector updates written with the same ownership need no barrier before the
+// next reduction.  pk_canon_sum adds each group's per-lane partial in k
+// order, then the groups in order, then a fixed shuffle tree, so the sum
+// depends on N alone, not on blockDim.  red: two buffers of 32 * ngroups
+// entries, alternated by `flip` (one barrier per sum).  All threads call it
+// and all get the sum.
 #define PK_CANON_GROUP 256
+#define PK_OWN_LOOP(k, N)                                                                      \
+    for (int _g = (int)(threadIdx.x >> 5); _g * PK_CANON_GROUP < (N); _g += (int)(blockDim.x >> 5)) \
+        for (int k = _g * PK_CANON_GROUP + (int)(threadIdx.x & 31);                             \
+             k < min((N), (_g + 1) * PK_CANON_GROUP); k += 32)
+
 template <typename T, typename Get>
-__device__ __forceinline__ T pk_canon_sum(int N, Get get, T* red)
+__device__ __forceinline__ T pk_canon_sum(int N, Get get, T* red, int& flip)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nw = blockDim.x >> 5;
     const int ng = (N + PK_CANON_GROUP - 1) / PK_CANON_GROUP;
+    T* buf = red + (flip ? 32 * ng : 0);
+    flip ^= 1;
     for (int grp = warp; grp < ng; grp += nw) {
         T s = T(0);
         const int end = min(N, (grp + 1) * PK_CANON_GROUP);
         for (int k = grp * PK_CANON_GROUP + lane; k < end; k += 32) s += get(k);
-        red[grp * 32 + lane] = s;
+        buf[grp * 32 + lane] = s;
     }
     __syncthreads();
     T r = T(0);
-    if (warp == 0) {
-        for (int grp = 0; grp < ng; ++grp) r += red[grp * 32 + lane];
-        r = pk_warp_sum(r);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) red[0] = r;
-    __syncthreads();
-    r = red[0];
-    __syncthreads();
-    return r;
+    for (int grp = 0; grp < ng; ++grp) r += buf[grp * 32 + lane];
+    return pk_warp_sum(r);
 }
 
-__host__ __device__ inline int pk_canon_red_len(int N) { return 32 * ((N + PK_CANON_GROUP - 1) / PK_CANON_GROUP + 1); }
+// Both buffers of pk_canon_sum (plus 32 entries of slack for block max).
+__host__ __device__ inline int pk_canon_red_len(int N) { return 2 * 32 * ((N + PK_CANON_GROUP - 1) / PK_CANON_GROUP) + 32; }
 
 // Bounded wrap of an angle difference into [-pi, pi], following the
 // reference's subtract-2pi loop (pack_cuda_lut.py:289-293) in FP32.  Angles

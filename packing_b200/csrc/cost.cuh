@@ -24,17 +24,32 @@ struct PkCostSmem {
     float4* aabb;       // [4*n_max] per piece: minx, maxx, miny, maxy (centre-relative)
     long long* acc;     // [3*n_max] fixed-point gradient
     float4* bnd;        // [n_max] boundary: cost, dh0, dh1, dh2 (unweighted)
-    uint32_t* items;    // [cap]
-    int* count;
+    uint32_t* items;    // [cap_items] piece pairs: i | j << 11 | pi << 22 | pj << 24
+    uint32_t* near;     // [cap_near] centre-culled pairs: i | j << 11
+    int* count;         // items in the list
+    int* count_near;    // near pairs in the list
     double* red;        // [32]
     long long* redl;    // [32]
     float2* piece;      // [16]
     int* piece_nv;      // [4]
     unsigned int* cnt;  // [4] enumerated pairs, near pairs, piece pairs, evaluations
-    int cap;
+    int cap_items, cap_near;
 };
 
-__host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap)
+// Pairs each thread tests per enumeration round.
+#define PK_PAIRS_PER_THREAD 8
+
+// List capacities: a round appends at most PK_PAIRS_PER_THREAD * T near
+// pairs, an expansion chunk at most 16 T piece pairs (T for the LUT, whose
+// items are the near pairs themselves); each list is flushed before the next
+// round could overflow it.
+__host__ __device__ inline void pk_caps(int T, int mode, int* cap_near, int* cap_items)
+{
+    *cap_near = 2 * PK_PAIRS_PER_THREAD * T;
+    *cap_items = mode == PK_PAIR_LUT ? 0 : 20 * T;
+}
+
+__host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap_near, int cap_items)
 {
     size_t b = 0;
     b += (size_t)n_max * 16;        // pose
@@ -42,12 +57,13 @@ __host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap)
     b += (size_t)n_max * 64;        // aabb
     b += (size_t)n_max * 24;        // acc
     b += (size_t)n_max * 4;         // theta
-    b += (size_t)cap * 4;           // items
-    b += 32 * 8 + 32 * 8 + 16 * 8 + 4 * 4 + 16 + 16;
+    b += (size_t)cap_items * 4;     // items
+    b += (size_t)cap_near * 4;      // near pairs
+    b += 32 * 8 + 32 * 8 + 16 * 8 + 4 * 4 + 16 + 16 + 16;
     return b;
 }
 
-__device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int cap)
+__device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int cap_near, int cap_items)
 {
     PkCostSmem s;
     unsigned char* p = base;
@@ -59,11 +75,14 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
     s.redl = (long long*)p; p += 32 * 8;
     s.piece = (float2*)p; p += 16 * 8;
     s.theta = (float*)p; p += (size_t)n_max * 4;
-    s.items = (uint32_t*)p; p += (size_t)cap * 4;
+    s.items = (uint32_t*)p; p += (size_t)cap_items * 4;
+    s.near = (uint32_t*)p; p += (size_t)cap_near * 4;
     s.piece_nv = (int*)p; p += 16;
     s.count = (int*)p; p += 16;
+    s.count_near = (int*)p; p += 16;
     s.cnt = (unsigned int*)p; p += 16;
-    s.cap = cap;
+    s.cap_items = cap_items;
+    s.cap_near = cap_near;
     return s;
 }
 
@@ -84,110 +103,111 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
 // P edge line is kept only if both run the same way, so a shared boundary
 // segment is counted once and touching pieces contribute zero.
 // ---------------------------------------------------------------------------
-// Near-collinear edges (all four endpoints within PK_COLLINEAR_TOL of the
+// Near-collinear edges (all four endpoints within 2e-6 tree units of the
 // other edge's line) are classified from the same four numbers on both
-// sides, so the P-side and Q-side decisions can never disagree.
-#define PK_COLLINEAR_TOL2 4e-12f   // (2e-6)^2, squared distance in tree units
+// passes, so the two passes can never disagree about a shared boundary.
+#define PK_COLLINEAR_TOL2 4e-12f   // (2e-6)^2
+
+// (b - a) x (c - a) with fixed rounding, so that the same four points give
+// the same value wherever it is evaluated.
+__device__ __forceinline__ float pk_cross3_rn(float2 a, float2 b, float2 c)
+{
+    return __fmaf_rn(b.x - a.x, c.y - a.y, -__fmul_rn(b.y - a.y, c.x - a.x));
+}
+
+// f[k][v] = cross(Y[k+1] - Y[k], X[v] - Y[k]): X's vertices against Y's
+// edge lines (>= 0 inside).
+__device__ __forceinline__ void pk_side_values(const float2 (&X)[4], const float2 (&Y)[4], float (&f)[4][4])
+{
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) f[k][v] = pk_cross3_rn(Y[k], Y[(k + 1) & 3], X[v]);
+}
+
+// Some edge line of Y has every vertex of X strictly outside: X and Y are
+// disjoint (separating axis), no boundary portion of either lies in the other.
+__device__ __forceinline__ bool pk_separated(const float (&f)[4][4], bool y_tri)
+{
+    bool sep = false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k == 3 && y_tri) continue;
+        sep = sep || (f[k][0] < 0.f && f[k][1] < 0.f && f[k][2] < 0.f && f[k][3] < 0.f);
+    }
+    return sep;
+}
+
+// One pass of the assembly: the portions of X's edges inside Y, added to A2
+// (twice the area) and to g (gradient of X's rigid pose about centre ctr).
+// f holds X's vertices against Y's lines.  KEEP_SAME_DIR: a collinear edge
+// of X is kept when it runs the same way as Y's (X = Q) or always dropped
+// (X = P).  Crossing parameters use the fast divide (relative error a few
+// ulp); the sign logic is branch-free so lanes stay converged.
+template <bool KEEP_SAME_DIR>
+__device__ __forceinline__ void pk_clip_pass(const float2 (&X)[4], bool x_tri, const float2 (&Y)[4], bool y_tri,
+                                             const float (&f)[4][4], float2 ctr, float& A2, float3& g)
+{
+    const float tiny = c_geom.coll_tiny;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        if (v == 3 && x_tri) break;
+        const float2 a = X[v], b = X[(v + 1) & 3];
+        float tin = 0.f, tout = 1.f;
+        bool empty = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k == 3 && y_tri) continue;
+            const float fa = f[k][v], fb = f[k][(v + 1) & 3];
+            if (fabsf(fa) <= tiny && fabsf(fb) <= tiny) {
+                const float2 ya = Y[k], yb = Y[(k + 1) & 3];
+                const float2 ey = make_float2(yb.x - ya.x, yb.y - ya.y), ex = make_float2(b.x - a.x, b.y - a.y);
+                const float ty = PK_COLLINEAR_TOL2 * __fmaf_rn(ey.x, ey.x, __fmul_rn(ey.y, ey.y));
+                const float tx = PK_COLLINEAR_TOL2 * __fmaf_rn(ex.x, ex.x, __fmul_rn(ex.y, ex.y));
+                const float ra = pk_cross3_rn(a, b, ya), rb = pk_cross3_rn(a, b, yb);
+                if (fa * fa <= ty && fb * fb <= ty && ra * ra <= tx && rb * rb <= tx) {
+                    if (!KEEP_SAME_DIR || ex.x * ey.x + ex.y * ey.y <= 0.f) empty = true;
+                    continue;
+                }
+            }
+            const bool ia = fa >= 0.f, ib = fb >= 0.f;
+            const float t = __fdividef(fa, fa - fb);
+            empty = empty || (!ia && !ib);
+            tout = (ia && !ib) ? fminf(tout, t) : tout;
+            tin = (!ia && ib) ? fmaxf(tin, t) : tin;
+        }
+        if (!empty && tin < tout) {
+            const float dt = tout - tin;
+            const float2 e = make_float2(b.x - a.x, b.y - a.y);
+            A2 += dt * pk_cross(a, b);
+            const float2 N = make_float2(dt * e.y, -dt * e.x);
+            const float tm = 0.5f * (tin + tout);
+            const float2 m = make_float2(a.x + tm * e.x - ctr.x, a.y + tm * e.y - ctr.y);
+            g.x += N.x;
+            g.y += N.y;
+            g.z += pk_cross(m, N);
+        }
+    }
+}
+
 __device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_tri,
                                                    const float2 (&Q)[4], bool q_tri, float2 d,
                                                    float& area, float3& gP, float3& gQ)
 {
-    float fPQ[4][4];   // [Q line k][P vertex v]
-    float fQP[4][4];   // [P line k][Q vertex v]
-    float tP[4], tQ[4];
-    float2 eP[4], eQ[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float2 qa = Q[k], qb = Q[(k + 1) & 3];
-        const float2 pa = P[k], pb = P[(k + 1) & 3];
-        eP[k] = make_float2(pb.x - pa.x, pb.y - pa.y);
-        eQ[k] = make_float2(qb.x - qa.x, qb.y - qa.y);
-        tP[k] = PK_COLLINEAR_TOL2 * (eP[k].x * eP[k].x + eP[k].y * eP[k].y);
-        tQ[k] = PK_COLLINEAR_TOL2 * (eQ[k].x * eQ[k].x + eQ[k].y * eQ[k].y);
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            fPQ[k][v] = pk_cross3(qa, qb, P[v]);
-            fQP[k][v] = pk_cross3(pa, pb, Q[v]);
-        }
-    }
     float A2 = 0.f;   // twice the area
     gP = make_float3(0.f, 0.f, 0.f);
     gQ = make_float3(0.f, 0.f, 0.f);
-    // Edges of P against Q's half-planes.
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        if (v == 3 && p_tri) continue;
-        const float2 a = P[v], b = P[(v + 1) & 3];
-        float tin = 0.f, tout = 1.f;
-        bool empty = false;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (k == 3 && q_tri) continue;
-            const float fa = fPQ[k][v], fb = fPQ[k][(v + 1) & 3];
-            const float ra = fQP[v][k], rb = fQP[v][(k + 1) & 3];
-            if (fa * fa <= tQ[k] && fb * fb <= tQ[k] && ra * ra <= tP[v] && rb * rb <= tP[v]) {
-                empty = true;   // collinear: the Q edge carries this boundary
-                continue;
-            }
-            const bool ia = fa >= 0.f, ib = fb >= 0.f;
-            if (!ia && !ib) {
-                empty = true;
-            } else if (ia != ib) {
-                const float t = fa / (fa - fb);
-                if (ia) tout = fminf(tout, t);
-                else tin = fmaxf(tin, t);
-            }
-        }
-        if (!empty && tin < tout) {
-            const float dt = tout - tin;
-            const float2 e = eP[v];
-            A2 += dt * pk_cross(a, b);
-            const float2 N = make_float2(dt * e.y, -dt * e.x);
-            const float tm = 0.5f * (tin + tout);
-            const float2 m = make_float2(a.x + tm * e.x, a.y + tm * e.y);
-            gP.x += N.x;
-            gP.y += N.y;
-            gP.z += pk_cross(m, N);
-        }
+    area = 0.f;
+    float f[4][4];
+    pk_side_values(P, Q, f);
+    if (pk_separated(f, q_tri)) return;
+    pk_clip_pass<false>(P, p_tri, Q, q_tri, f, make_float2(0.f, 0.f), A2, gP);
+    pk_side_values(Q, P, f);
+    if (pk_separated(f, p_tri)) {
+        gP = make_float3(0.f, 0.f, 0.f);
+        return;
     }
-    // Edges of Q against P's half-planes.
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-        if (v == 3 && q_tri) continue;
-        const float2 a = Q[v], b = Q[(v + 1) & 3];
-        const float2 e = eQ[v];
-        float tin = 0.f, tout = 1.f;
-        bool empty = false;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (k == 3 && p_tri) continue;
-            const float fa = fQP[k][v], fb = fQP[k][(v + 1) & 3];
-            const float ra = fPQ[v][k], rb = fPQ[v][(k + 1) & 3];
-            if (fa * fa <= tP[k] && fb * fb <= tP[k] && ra * ra <= tQ[v] && rb * rb <= tQ[v]) {
-                // collinear: kept (no constraint) when both run the same way
-                if (eP[k].x * e.x + eP[k].y * e.y <= 0.f) empty = true;
-                continue;
-            }
-            const bool ia = fa >= 0.f, ib = fb >= 0.f;
-            if (!ia && !ib) {
-                empty = true;
-            } else if (ia != ib) {
-                const float t = fa / (fa - fb);
-                if (ia) tout = fminf(tout, t);
-                else tin = fmaxf(tin, t);
-            }
-        }
-        if (!empty && tin < tout) {
-            const float dt = tout - tin;
-            A2 += dt * pk_cross(a, b);
-            const float2 N = make_float2(dt * e.y, -dt * e.x);
-            const float tm = 0.5f * (tin + tout);
-            const float2 m = make_float2(a.x + tm * e.x - d.x, a.y + tm * e.y - d.y);
-            gQ.x += N.x;
-            gQ.y += N.y;
-            gQ.z += pk_cross(m, N);
-        }
-    }
+    pk_clip_pass<true>(Q, q_tri, P, p_tri, f, d, A2, gQ);
     area = 0.5f * A2;
     if (!(area > 0.f)) {   // empty or numerically vanishing overlap
         area = 0.f;
@@ -344,12 +364,12 @@ __device__ __forceinline__ void pk_load_piece(const PkCostSmem& sm, int p, float
 // Phase B: evaluate every listed item; returns this thread's fixed-point
 // pair total.  Items: i (11 bits) | j (11 bits) | pi (2) | pj (2).
 template <int MODE>
-__device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, int count, float w_pair,
-                                                      const PkLut& lut)
+__device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, const uint32_t* list, int count,
+                                                      float w_pair, const PkLut& lut)
 {
     long long tot = 0;
     for (int w = threadIdx.x; w < count; w += blockDim.x) {
-        const uint32_t it = sm.items[w];
+        const uint32_t it = list[w];
         const int i = it & 2047, j = (it >> 11) & 2047;
         const float4 A = sm.pose[i], B = sm.pose[j];
         const float2 d = make_float2(B.x - A.x, B.y - A.y);
@@ -504,6 +524,7 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
     }
     if (threadIdx.x == 0) {
         *sm.count = 0;
+        *sm.count_near = 0;
         sm.cnt[3] += 1;
         if (MODE != PK_PAIR_NONE && n > 1) sm.cnt[0] += (unsigned)(n * (n - 1) / 2);
     }
@@ -515,67 +536,104 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
         const int npairs = n * (n - 1) / 2;
         const float cutoff = c_geom.cutoff_sq;
         const int lane = threadIdx.x & 31;
-        const int per_round = (MODE == PK_PAIR_LUT) ? T : 16 * T;
-        for (int base = 0; base < npairs; base += T) {
-            const int k = base + threadIdx.x;
-            uint32_t mask = 0;
-            int i = 0, j = 0;
-            if (k < npairs) {
-                // pair k: distance class dd = k / n + 1, i = k mod n, j = (i + dd) mod n
-                const int dd = k / n;
-                i = k - dd * n;
-                j = i + dd + 1;
-                if (j >= n) j -= n;
-                const float4 A = sm.pose[i], B = sm.pose[j];
-                const float dx = B.x - A.x, dy = B.y - A.y;
-                if (dx * dx + dy * dy <= cutoff) {
-                    if (MODE == PK_PAIR_LUT) {
-                        mask = 1;
-                    } else {
+        const unsigned lt = (1u << lane) - 1u;
+        const int span = PK_PAIRS_PER_THREAD * T;
+        // pair k = dd * n + i -> (i, (i + dd + 1) mod n); this thread's k
+        // advances by T, so (dd, i) advance by (T / n, T % n) with one carry
+        const int tdiv = T / n, tmod = T - (T / n) * n;
+        int cdd = threadIdx.x / n, ci = threadIdx.x - (threadIdx.x / n) * n;
+        for (int base = 0; base < npairs; base += span) {
+            // enumeration: PK_PAIRS_PER_THREAD pairs per thread, centre cull,
+            // survivors appended to the near list (one shared atomic per warp)
 #pragma unroll
-                        for (int p = 0; p < 4; ++p) {
-                            const float4 a = sm.aabb[4 * i + p];
+            for (int r = 0; r < PK_PAIRS_PER_THREAD; ++r) {
+                const int k = base + r * T + threadIdx.x;
+                bool nr = false;
+                uint32_t ij = 0;
+                const int i = ci;
+                int j = i + cdd + 1;
+                ci += tmod;
+                cdd += tdiv;
+                if (ci >= n) { ci -= n; ++cdd; }
+                if (k < npairs) {
+                    if (j >= n) j -= n;
+                    const float4 A = sm.pose[i], B = sm.pose[j];
+                    const float dx = B.x - A.x, dy = B.y - A.y;
+                    nr = dx * dx + dy * dy <= cutoff;
+                    ij = (uint32_t)i | ((uint32_t)j << 11);
+                }
+                const unsigned bal = __ballot_sync(PK_FULL_MASK, nr);
+                if (bal) {
+                    int wbase = 0;
+                    if (lane == 0) wbase = atomicAdd(sm.count_near, __popc(bal));
+                    wbase = __shfl_sync(PK_FULL_MASK, wbase, 0);
+                    if (nr) sm.near[wbase + __popc(bal & lt)] = ij;
+                }
+            }
+            __syncthreads();
+            const int cn = *sm.count_near;
+            __syncthreads();   // every thread has read the count before anyone appends again
+            if (cn > sm.cap_near - span || base + span >= npairs) {
+                if (threadIdx.x == 0) sm.cnt[1] += (unsigned)cn;
+                if (MODE == PK_PAIR_LUT) {
+                    // LUT items are the near pairs themselves
+                    if (threadIdx.x == 0) sm.cnt[2] += (unsigned)cn;
+                    pair_tot += pk_process_items<MODE>(sm, sm.near, cn, spec.w_pair, spec.lut);
+                } else {
+                    // expansion: 16 piece-pair AABB tests per near pair
+                    for (int c0 = 0; c0 < cn; c0 += T) {
+                        const int w = c0 + threadIdx.x;
+                        uint32_t mask = 0, ij = 0;
+                        if (w < cn) {
+                            ij = sm.near[w];
+                            const int i = ij & 2047, j = (ij >> 11) & 2047;
+                            const float4 A = sm.pose[i], B = sm.pose[j];
+                            const float dx = B.x - A.x, dy = B.y - A.y;
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                const float4 b = sm.aabb[4 * j + q];
-                                const bool ov = !(a.y < b.x + dx || b.y + dx < a.x || a.w < b.z + dy ||
-                                                  b.w + dy < a.z);
-                                mask |= (uint32_t)ov << (4 * p + q);
+                            for (int p = 0; p < 4; ++p) {
+                                const float4 a = sm.aabb[4 * i + p];
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    const float4 b = sm.aabb[4 * j + q];
+                                    const bool ov = !(a.y < b.x + dx || b.y + dx < a.x || a.w < b.z + dy ||
+                                                      b.w + dy < a.z);
+                                    mask |= (uint32_t)ov << (4 * p + q);
+                                }
                             }
+                        }
+                        const int cnt = __popc(mask);
+                        int incl = cnt;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const int v = __shfl_up_sync(PK_FULL_MASK, incl, o);
+                            if (lane >= o) incl += v;
+                        }
+                        const int wtot = __shfl_sync(PK_FULL_MASK, incl, 31);
+                        int wbase = 0;
+                        if (lane == 31 && wtot) {
+                            wbase = atomicAdd(sm.count, wtot);
+                            atomicAdd(&sm.cnt[2], (unsigned)wtot);
+                        }
+                        wbase = __shfl_sync(PK_FULL_MASK, wbase, 31);
+                        int pos = wbase + incl - cnt;
+                        while (mask) {
+                            const int b = __ffs(mask) - 1;
+                            mask &= mask - 1;
+                            sm.items[pos++] = ij | ((uint32_t)(b >> 2) << 22) | ((uint32_t)(b & 3) << 24);
+                        }
+                        __syncthreads();
+                        const int ci = *sm.count;
+                        __syncthreads();
+                        if (ci > sm.cap_items - 16 * T || c0 + T >= cn) {
+                            pair_tot += pk_process_items<MODE>(sm, sm.items, ci, spec.w_pair, spec.lut);
+                            __syncthreads();
+                            if (threadIdx.x == 0) *sm.count = 0;
+                            __syncthreads();
                         }
                     }
                 }
-            }
-            const int cnt = __popc(mask);
-            int incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(PK_FULL_MASK, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const int wtot = __shfl_sync(PK_FULL_MASK, incl, 31);
-            const unsigned nnear = __popc(__ballot_sync(PK_FULL_MASK, mask != 0));
-            int wbase = 0;
-            if (lane == 31 && wtot) {
-                wbase = atomicAdd(sm.count, wtot);
-                atomicAdd(&sm.cnt[1], nnear);
-                atomicAdd(&sm.cnt[2], (unsigned)wtot);
-            }
-            wbase = __shfl_sync(PK_FULL_MASK, wbase, 31);
-            int pos = wbase + incl - cnt;
-            const uint32_t ij = (uint32_t)i | ((uint32_t)j << 11);
-            while (mask) {
-                const int b = __ffs(mask) - 1;
-                mask &= mask - 1;
-                sm.items[pos++] = ij | ((uint32_t)(b >> 2) << 22) | ((uint32_t)(b & 3) << 24);
-            }
-            __syncthreads();
-            const int count = *sm.count;
-            __syncthreads();   // every thread has read count before the next round appends
-            if (count > sm.cap - per_round || base + T >= npairs) {
-                pair_tot += pk_process_items<MODE>(sm, count, spec.w_pair, spec.lut);
                 __syncthreads();
-                if (threadIdx.x == 0) *sm.count = 0;
+                if (threadIdx.x == 0) *sm.count_near = 0;
                 __syncthreads();
             }
         }
@@ -617,10 +675,10 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
 }
 
 template <int MODE>
-__global__ void pk_cost_kernel(const float* __restrict__ xyt, const int* __restrict__ offsets, int E,
+__global__ void __launch_bounds__(256, 3) pk_cost_kernel(const float* __restrict__ xyt, const int* __restrict__ offsets, int E,
                                int n_max, const float* __restrict__ h, PkCostSpec spec,
                                float* __restrict__ cost, float* __restrict__ grad,
-                               float* __restrict__ grad_h, int cap)
+                               float* __restrict__ grad_h, int cap_near, int cap_items)
 {
     extern __shared__ __align__(16) unsigned char pk_smem[];
     const int e = blockIdx.x;
@@ -631,7 +689,7 @@ __global__ void pk_cost_kernel(const float* __restrict__ xyt, const int* __restr
         if (threadIdx.x == 0) cost[e] = __int_as_float(0x7fc00000);   // NaN marks a bad offset
         return;
     }
-    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap);
+    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap_near, cap_items);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
     __syncthreads();
     const double tot = pk_eval_instance<MODE>(xyt + (size_t)base * 3, n, h ? h + 3 * e : nullptr, spec,
@@ -649,9 +707,6 @@ static inline int pk_cost_threads(int n_max)
     return 256;
 }
 
-// Item-list capacity: one round appends at most T (LUT) or 16 T items and the
-// list is flushed before it could overflow, so cap must exceed that bound.
-static inline int pk_cost_cap(int T, int mode) { return mode == PK_PAIR_LUT ? 4 * T : 24 * T; }
 
 static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max, const float* h,
                           const PkCostSpec* spec, float* cost, float* grad, float* grad_h,
@@ -672,8 +727,9 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
             return pk_fail(PK_EINVAL, "pk_cost: LUT needs vals and at least 2 points per axis%s");
     }
     const int T = pk_cost_threads(n_max);
-    const int cap = pk_cost_cap(T, spec->pair_mode);
-    const size_t smem = pk_cost_smem_bytes(n_max, cap);
+    int cap_near, cap_items;
+    pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
+    const size_t smem = pk_cost_smem_bytes(n_max, cap_near, cap_items);
     cudaError_t err = cudaSuccess;
     switch (spec->pair_mode) {
 #define PK_CASE(M)                                                                                  \
@@ -682,7 +738,7 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
                                    (int)smem);                                                      \
         if (err == cudaSuccess) {                                                                   \
             pk_cost_kernel<M><<<E, T, smem, st>>>(xyt, offsets, E, n_max, h, *spec, cost, grad,     \
-                                                  grad_h, cap);                                     \
+                                                  grad_h, cap_near, cap_items);                     \
             err = cudaGetLastError();                                                               \
         }                                                                                           \
         break;

@@ -140,6 +140,15 @@ extern "C" int pk_init(const PkGeometry* geom_in)
     if (g.max_radius > rmax) rmax = g.max_radius;
     d.n_tree = g.n_tree_verts;
     d64.n_tree = g.n_tree_verts;
+    double emax = 0.0;
+    for (int p = 0; p < PK_NUM_PIECES; ++p)
+        for (int k = 0; k < 4; ++k) {
+            const double ex = d64.piece[p][(k + 1) & 3].x - d64.piece[p][k].x;
+            const double ey = d64.piece[p][(k + 1) & 3].y - d64.piece[p][k].y;
+            const double l = sqrt(ex * ex + ey * ey);
+            emax = l > emax ? l : emax;
+        }
+    d.coll_tiny = (float)(2.0e-6 * emax * 1.01);
     d.max_radius = (float)rmax;
     d.cutoff_sq = (float)((2.0 * rmax) * (2.0 * rmax));
     d64.max_radius = rmax;

@@ -8,6 +8,8 @@
 //    the gradient and the direction in shared memory, evaluates the compound
 //    cost with the cost kernel's device code and iterates to max_iter in a
 //    single launch.
+// Both use the same order-fixed reductions (pk_canon_sum), so given the same
+// objective values they produce the same iterates bit for bit.
 // History is a ring buffer (logical entry i of a system lives in slot
 // (start + i) % m), which is equivalent to the reference's shift-left-and-
 // append (:676-690) without moving memory.
@@ -16,39 +18,43 @@
 #include "cost.cuh"
 
 template <typename F>
-__device__ __forceinline__ F pk_bsum(F v, F* red) { return pk_block_sum<F>(v, red); }
-
-template <typename F>
 __device__ __forceinline__ F pk_bmax(F v, F* red) { return pk_block_max<F>(v, red); }
 
 // Two-loop recursion (:533-572) for one system: d = -H g with the valid
 // history entries in logical order; al is shared scratch of m entries.
+// Vector work uses element ownership (PK_OWN_LOOP): no barrier besides the
+// one inside each reduction.
 template <typename F>
 __device__ void pk_two_loop(const F* g, F* d, int N, const F* S, const F* Y, const F* ro, int m, int hlen,
-                            int hstart, F Hdiag, F* al, F* red)
+                            int hstart, F Hdiag, F* al, F* red, int& flip)
 {
-    for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = -g[k];
-    __syncthreads();
+    PK_OWN_LOOP(k, N) d[k] = -g[k];
     for (int i = hlen - 1; i >= 0; --i) {
         const int slot = (hstart + i) % m;
         const F* s = S + (size_t)slot * N;
         const F* y = Y + (size_t)slot * N;
-        const F a = pk_canon_sum<F>(N, [&](int k) { return s[k] * d[k]; }, red) * ro[slot];
+        const F a = pk_canon_sum<F>(N, [&](int k) { return s[k] * d[k]; }, red, flip) * ro[slot];
         if (threadIdx.x == 0) al[i] = a;
-        for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = d[k] - y[k] * a;
-        __syncthreads();
+        PK_OWN_LOOP(k, N) d[k] = d[k] - y[k] * a;
     }
-    for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = d[k] * Hdiag;
-    __syncthreads();
+    PK_OWN_LOOP(k, N) d[k] = d[k] * Hdiag;
+    __syncthreads();   // al[] visible
     for (int i = 0; i < hlen; ++i) {
         const int slot = (hstart + i) % m;
         const F* s = S + (size_t)slot * N;
         const F* y = Y + (size_t)slot * N;
-        const F be = pk_canon_sum<F>(N, [&](int k) { return y[k] * d[k]; }, red) * ro[slot];
+        const F be = pk_canon_sum<F>(N, [&](int k) { return y[k] * d[k]; }, red, flip) * ro[slot];
         const F c = al[i] - be;
-        for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = d[k] + s[k] * c;
-        __syncthreads();
+        PK_OWN_LOOP(k, N) d[k] = d[k] + s[k] * c;
     }
+}
+
+template <typename F>
+__device__ __forceinline__ F pk_own_absmax(int N, const F* v, F scale, F* red)
+{
+    F p = 0;
+    PK_OWN_LOOP(k, N) p = fmax(p, (F)fabs(v[k] * scale));
+    return pk_bmax<F>(p, red + 2 * 32 * ((N + PK_CANON_GROUP - 1) / PK_CANON_GROUP));
 }
 
 // ---------------------------------------------------------------------------
@@ -73,6 +79,7 @@ __global__ void pk_lbfgs_direction_kernel(PkLbfgsState<F> s, int n_iter, F lr, F
     const int N = s.N;
     F* al = (F*)pk_smem;
     F* red = al + s.m;
+    int flip = 0;
     const int b = blockIdx.x;
     const F* g = s.g + (size_t)b * N;
     F* d = s.d + (size_t)b * N;
@@ -80,17 +87,16 @@ __global__ void pk_lbfgs_direction_kernel(PkLbfgsState<F> s, int n_iter, F lr, F
     int active = s.active[b];
     F Hd = s.H[b];
     if (n_iter == 1) {
-        for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = -g[k];
+        PK_OWN_LOOP(k, N) d[k] = -g[k];
         Hd = 1;
-        __syncthreads();
     } else {
         pk_two_loop<F>(g, d, N, s.S + (size_t)b * s.m * N, s.Y + (size_t)b * s.m * N, s.ro + (size_t)b * s.m, s.m,
-                       s.hlen[b], s.hstart[b], Hd, al, red);
+                       s.hlen[b], s.hstart[b], Hd, al, red, flip);
     }
-    for (int k = threadIdx.x; k < N; k += blockDim.x) pg[k] = g[k];
+    PK_OWN_LOOP(k, N) pg[k] = g[k];
     F t;
     if (n_iter == 1) {
-        const F gs = pk_canon_sum<F>(N, [&](int k) { return (F)fabs(g[k]); }, red);
+        const F gs = pk_canon_sum<F>(N, [&](int k) { return (F)fabs(g[k]); }, red, flip);
         t = (F)1 / gs;
         t = (t < (F)1 ? t : (F)1) * lr;   // torch.minimum(1, 1/sum|g|) * lr
         if (!active) t = 0;
@@ -98,12 +104,10 @@ __global__ void pk_lbfgs_direction_kernel(PkLbfgsState<F> s, int n_iter, F lr, F
         t = lr;
     }
     if (has_max_step) {
-        F part = 0;
-        for (int k = threadIdx.x; k < N; k += blockDim.x) part = fmax(part, fabs(d[k] * t));
-        const F pc = pk_bmax<F>(part, red);
+        const F pc = pk_own_absmax<F>(N, d, t, red);
         if (pc > max_step) t = t * (max_step / pc);
     }
-    const F gtd = pk_canon_sum<F>(N, [&](int k) { return g[k] * d[k]; }, red);
+    const F gtd = pk_canon_sum<F>(N, [&](int k) { return g[k] * d[k]; }, red, flip);
     if (gtd > -tol_change) active = 0;
     if (threadIdx.x == 0) {
         s.t[b] = t;
@@ -133,6 +137,7 @@ __global__ void pk_lbfgs_update_kernel(PkLbfgsState<F> s, int n_iter, F tol_grad
 {
     extern __shared__ __align__(16) unsigned char pk_smem[];
     F* red = (F*)pk_smem;
+    int flip = 0;
     const int b = blockIdx.x;
     const int N = s.N, m = s.m;
     const F* g = s.g + (size_t)b * N;
@@ -142,15 +147,15 @@ __global__ void pk_lbfgs_update_kernel(PkLbfgsState<F> s, int n_iter, F tol_grad
     int active = s.active[b];
     int evals = s.evals[b] + 1;
     if (n_iter > 1) {
-        const F ys = pk_canon_sum<F>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red);
-        const F yy = pk_canon_sum<F>(N, [&](int k) { const F y = g[k] - pg[k]; return y * y; }, red);
+        const F ys = pk_canon_sum<F>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red, flip);
+        const F yy = pk_canon_sum<F>(N, [&](int k) { const F y = g[k] - pg[k]; return y * y; }, red, flip);
         if (active && ys > (F)1e-10) {
             int hl = s.hlen[b], hs = s.hstart[b], slot;
             if (hl < m) { slot = (hs + hl) % m; ++hl; }
             else { slot = hs; hs = (hs + 1) % m; }
             F* S = s.S + ((size_t)b * m + slot) * N;
             F* Y = s.Y + ((size_t)b * m + slot) * N;
-            for (int k = threadIdx.x; k < N; k += blockDim.x) {
+            PK_OWN_LOOP(k, N) {
                 Y[k] = g[k] - pg[k];
                 S[k] = d[k] * t;
             }
@@ -162,13 +167,8 @@ __global__ void pk_lbfgs_update_kernel(PkLbfgsState<F> s, int n_iter, F tol_grad
             }
         }
     }
-    F pmx = 0, pch = 0;
-    for (int k = threadIdx.x; k < N; k += blockDim.x) {
-        pmx = fmax(pmx, fabs(g[k]));
-        pch = fmax(pch, fabs(d[k] * t));
-    }
-    const F gmax = pk_bmax<F>(pmx, red);
-    const F pc = pk_bmax<F>(pch, red);
+    const F gmax = pk_own_absmax<F>(N, g, (F)1, red);
+    const F pc = pk_own_absmax<F>(N, d, t, red);
     if (threadIdx.x == 0) {
         if (gmax <= tol_grad) active = 0;
         if (evals >= max_eval) active = 0;
@@ -192,10 +192,7 @@ __global__ void pk_lbfgs_init_kernel(PkLbfgsState<F> s, F tol_grad)
     extern __shared__ __align__(16) unsigned char pk_smem[];
     F* red = (F*)pk_smem;
     const int b = blockIdx.x;
-    const F* g = s.g + (size_t)b * s.N;
-    F p = 0;
-    for (int k = threadIdx.x; k < s.N; k += blockDim.x) p = fmax(p, fabs(g[k]));
-    const F gm = pk_bmax<F>(p, red);
+    const F gm = pk_own_absmax<F>(s.N, s.g + (size_t)b * s.N, (F)1, red);
     if (threadIdx.x == 0) {
         const int a = gm <= tol_grad ? 0 : 1;
         s.active[b] = a;
@@ -217,16 +214,27 @@ static int pk_lbfgs_phase(int phase, const PkLbfgsState<F>& s, int n_iter, doubl
     const int T = pk_lbfgs_threads(s.N);
     const size_t smem = ((size_t)s.m + pk_canon_red_len(s.N)) * sizeof(F);
     if (s.M == 0) return PK_OK;
+    cudaError_t err = cudaSuccess;
     switch (phase) {
-        case 0: pk_lbfgs_init_kernel<F><<<s.M, T, smem, st>>>(s, (F)a); break;
-        case 1: pk_lbfgs_direction_kernel<F><<<s.M, T, smem, st>>>(s, n_iter, (F)a, (F)b_, i1, (F)c); break;
+        case 0:
+        case 1:
+        case 3: {
+            const void* fn = phase == 0 ? (const void*)pk_lbfgs_init_kernel<F>
+                           : phase == 1 ? (const void*)pk_lbfgs_direction_kernel<F>
+                                        : (const void*)pk_lbfgs_update_kernel<F>;
+            err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (err != cudaSuccess) return pk_cuda_check(err, "pk_lbfgs attribute");
+            if (phase == 0) pk_lbfgs_init_kernel<F><<<s.M, T, smem, st>>>(s, (F)a);
+            else if (phase == 1) pk_lbfgs_direction_kernel<F><<<s.M, T, smem, st>>>(s, n_iter, (F)a, (F)b_, i1, (F)c);
+            else pk_lbfgs_update_kernel<F><<<s.M, T, smem, st>>>(s, n_iter, (F)a, (F)b_, (F)c, i1, i2);
+            break;
+        }
         case 2: {
             const size_t total = (size_t)s.M * s.N;
             const int blocks = (int)((total + 255) / 256 < 148 * 8 ? (total + 255) / 256 : 148 * 8);
             pk_lbfgs_step_kernel<F><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(s.x, s.d, s.t, s.M, s.N);
             break;
         }
-        case 3: pk_lbfgs_update_kernel<F><<<s.M, T, smem, st>>>(s, n_iter, (F)a, (F)b_, (F)c, i1, i2); break;
         default: return pk_fail(PK_EINVAL, "pk_lbfgs: unknown phase%s");
     }
     (void)d_;
@@ -265,14 +273,15 @@ extern "C" int pk_lbfgs_phase(int phase, int dtype_bytes, void* const* arrays, i
 // pack_dynamics.py:76-83.  Per-instance stop: an instance that becomes
 // inactive stops stepping (the reference keeps stepping inactive systems
 // while another system of the same batch is still active, so with this form
-// an instance's result never depends on the rest of the batch).
+// an instance's result never depends on the rest of the batch).  The cost is
+// evaluated at one place in the loop (smaller code than one copy per use).
 // ---------------------------------------------------------------------------
 template <int MODE>
-__global__ void pk_relax_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in,
+__global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in,
                                 const int* __restrict__ offsets, const int* __restrict__ order, int E, int n_max,
                                 PkCostSpec spec, PkRelaxParams prm, float* __restrict__ xyt_out,
                                 float* __restrict__ h_out, float* __restrict__ loss_out, int* __restrict__ iters_out,
-                                float* __restrict__ work, int cap)
+                                float* __restrict__ work, int cap_near, int cap_items)
 {
     extern __shared__ __align__(16) unsigned char pk_smem[];
     const int e = order ? order[blockIdx.x] : blockIdx.x;
@@ -286,110 +295,106 @@ __global__ void pk_relax_kernel(const float* __restrict__ xyt_in, const float* _
     const int N = 3 * n + 3;
     const int NM = 3 * n_max + 3;
     const int m = prm.history;
-    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap);
+    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap_near, cap_items);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
-    float* x = (float*)(pk_smem + pk_cost_smem_bytes(n_max, cap));
+    float* x = (float*)(pk_smem + pk_cost_smem_bytes(n_max, cap_near, cap_items));
     float* g = x + NM;
     float* pg = g + NM;
     float* d = pg + NM;
     float* al = d + NM;
     float* ro = al + m;
     float* red = ro + m;
+    int flip = 0;
     // history of this instance: work + 2 m * (3 * base + 3 * e) floats
     float* S = work + (size_t)2 * m * (3 * (size_t)base + 3 * (size_t)e);
     float* Y = S + (size_t)m * N;
     for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) x[k] = xyt_in[(size_t)base * 3 + k];
     if (threadIdx.x < 3) x[3 * n + threadIdx.x] = h_in ? h_in[3 * e + threadIdx.x] : 0.f;
-    __syncthreads();
+    if (threadIdx.x < 3) g[3 * n + threadIdx.x] = 0.f;
     const bool use_h = h_in != nullptr;
-    double L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, g, use_h ? g + 3 * n : nullptr, sm);
-    if (!use_h && threadIdx.x < 3) g[3 * n + threadIdx.x] = 0.f;
-    __syncthreads();
-    float loss = (float)L;
-    const float loss0 = loss;
-    float gm = 0.f;
-    for (int k = threadIdx.x; k < N; k += blockDim.x) gm = fmaxf(gm, fabsf(g[k]));
-    gm = pk_bmax<float>(gm, red);
-    bool active = !(gm <= prm.tol_grad);
+    float loss = 0.f, loss0 = 0.f, ploss = 0.f, H = 1.f, t = 0.f;
     int evals = 1, hlen = 0, hstart = 0, it = 0;
     unsigned long long hist_streamed = 0;
-    float H = 1.f;
-    while (active && it < prm.max_iter) {
+    bool active = true, need_eval = true, final_pending = false, want_grad = true;
+    for (;;) {
+        if (need_eval) {
+            __syncthreads();   // x complete
+            const double L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, want_grad ? g : nullptr,
+                                                    (want_grad && use_h) ? g + 3 * n : nullptr, sm);
+            loss = (float)L;
+        }
+        if (final_pending) break;
+        if (it == 0) {
+            // initial point (:489-500)
+            loss0 = loss;
+            const float gm = pk_own_absmax<float>(N, g, 1.f, red);
+            active = !(gm <= prm.tol_grad);
+        } else {
+            // after a step (:632-724)
+            ++evals;
+            if (it > 1) {
+                const float ys = pk_canon_sum<float>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red, flip);
+                const float yy = pk_canon_sum<float>(N, [&](int k) { const float y = g[k] - pg[k]; return y * y; },
+                                                     red, flip);
+                if (ys > 1e-10f) {
+                    int slot;
+                    if (hlen < m) { slot = (hstart + hlen) % m; ++hlen; }
+                    else { slot = hstart; hstart = (hstart + 1) % m; }
+                    float* Sd = S + (size_t)slot * N;
+                    float* Yd = Y + (size_t)slot * N;
+                    PK_OWN_LOOP(k, N) {
+                        Yd[k] = g[k] - pg[k];
+                        Sd[k] = d[k] * t;
+                    }
+                    H = ys / yy;
+                    if (threadIdx.x == 0) ro[slot] = 1.f / ys;
+                }
+            }
+            const float gmax = pk_own_absmax<float>(N, g, 1.f, red);
+            const float pc = pk_own_absmax<float>(N, d, t, red);
+            if (gmax <= prm.tol_grad) active = false;
+            if (evals >= prm.max_eval) active = false;
+            if (pc <= prm.tol_change) active = false;
+            const float lc = fabsf(loss - ploss);
+            if (lc < prm.tol_change) active = false;
+            if (prm.tol_rel_change > 0.f && it > m && lc / (fabsf(ploss) + 1e-12f) < prm.tol_rel_change) active = false;
+            if (prm.stop_on_cost_increase && loss > loss0) active = false;
+        }
+        if (!active || it >= prm.max_iter) break;
+        // ---- next step (:531-631) ----
         ++it;
         if (it == 1) {
-            for (int k = threadIdx.x; k < N; k += blockDim.x) d[k] = -g[k];
+            PK_OWN_LOOP(k, N) d[k] = -g[k];
             H = 1.f;
-            __syncthreads();
         } else {
-            pk_two_loop<float>(g, d, N, S, Y, ro, m, hlen, hstart, H, al, red);
+            pk_two_loop<float>(g, d, N, S, Y, ro, m, hlen, hstart, H, al, red, flip);
             hist_streamed += (unsigned long long)hlen;
         }
-        for (int k = threadIdx.x; k < N; k += blockDim.x) pg[k] = g[k];
-        const float ploss = loss;
-        float t;
+        PK_OWN_LOOP(k, N) pg[k] = g[k];
+        ploss = loss;
         if (it == 1) {
-            const float gs = pk_canon_sum<float>(N, [&](int k) { return fabsf(g[k]); }, red);
+            const float gs = pk_canon_sum<float>(N, [&](int k) { return fabsf(g[k]); }, red, flip);
             t = 1.f / gs;
             t = (t < 1.f ? t : 1.f) * prm.lr;
         } else {
             t = prm.lr;
         }
         if (prm.has_max_step) {
-            float p = 0.f;
-            for (int k = threadIdx.x; k < N; k += blockDim.x) p = fmaxf(p, fabsf(d[k] * t));
-            const float pc = pk_bmax<float>(p, red);
+            const float pc = pk_own_absmax<float>(N, d, t, red);
             if (pc > prm.max_step) t = t * (prm.max_step / pc);
         }
-        {
-            const float gtd = pk_canon_sum<float>(N, [&](int k) { return g[k] * d[k]; }, red);
-            if (gtd > -prm.tol_change) { active = false; --it; break; }
+        const float gtd = pk_canon_sum<float>(N, [&](int k) { return g[k] * d[k]; }, red, flip);
+        if (gtd > -prm.tol_change) { active = false; --it; break; }
+        PK_OWN_LOOP(k, N) x[k] = x[k] + t * d[k];
+        need_eval = it != prm.max_iter;
+        if (!need_eval && prm.final_eval) {
+            // the last step is not evaluated by the reference loop; evaluate once for loss_out
+            need_eval = true;
+            want_grad = false;
+            final_pending = true;
         }
-        for (int k = threadIdx.x; k < N; k += blockDim.x) x[k] = x[k] + t * d[k];
-        __syncthreads();
-        if (it != prm.max_iter) {
-            L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, g, use_h ? g + 3 * n : nullptr, sm);
-            loss = (float)L;
-            if (!use_h && threadIdx.x < 3) g[3 * n + threadIdx.x] = 0.f;
-            __syncthreads();
-        }
-        ++evals;
-        if (it > 1) {
-            const float ys = pk_canon_sum<float>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red);
-            const float yy = pk_canon_sum<float>(N, [&](int k) { const float y = g[k] - pg[k]; return y * y; }, red);
-            if (ys > 1e-10f) {
-                int slot;
-                if (hlen < m) { slot = (hstart + hlen) % m; ++hlen; }
-                else { slot = hstart; hstart = (hstart + 1) % m; }
-                float* Sd = S + (size_t)slot * N;
-                float* Yd = Y + (size_t)slot * N;
-                for (int k = threadIdx.x; k < N; k += blockDim.x) {
-                    Yd[k] = g[k] - pg[k];
-                    Sd[k] = d[k] * t;
-                }
-                H = ys / yy;
-                if (threadIdx.x == 0) ro[slot] = 1.f / ys;
-                __syncthreads();
-            }
-        }
-        float pmx = 0.f, pch = 0.f;
-        for (int k = threadIdx.x; k < N; k += blockDim.x) {
-            pmx = fmaxf(pmx, fabsf(g[k]));
-            pch = fmaxf(pch, fabsf(d[k] * t));
-        }
-        const float gmax = pk_bmax<float>(pmx, red);
-        const float pc = pk_bmax<float>(pch, red);
-        if (gmax <= prm.tol_grad) active = false;
-        if (evals >= prm.max_eval) active = false;
-        if (pc <= prm.tol_change) active = false;
-        const float lc = fabsf(loss - ploss);
-        if (lc < prm.tol_change) active = false;
-        if (prm.tol_rel_change > 0.f && it > m && lc / (fabsf(ploss) + 1e-12f) < prm.tol_rel_change) active = false;
-        if (prm.stop_on_cost_increase && loss > loss0) active = false;
     }
-    if (prm.final_eval) {
-        L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, nullptr, nullptr, sm);
-        loss = (float)L;
-    }
+    __syncthreads();
     for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) xyt_out[(size_t)base * 3 + k] = x[k];
     if (h_out && threadIdx.x < 3) h_out[3 * e + threadIdx.x] = x[3 * n + threadIdx.x];
     if (threadIdx.x == 0) {
@@ -403,10 +408,10 @@ __global__ void pk_relax_kernel(const float* __restrict__ xyt_in, const float* _
     }
 }
 
-static size_t pk_relax_smem_bytes(int n_max, int cap, int m)
+static size_t pk_relax_smem_bytes(int n_max, int cap_near, int cap_items, int m)
 {
     const int NM = 3 * n_max + 3;
-    return pk_cost_smem_bytes(n_max, cap) + ((size_t)4 * NM + 2 * (size_t)m + pk_canon_red_len(NM)) * 4;
+    return pk_cost_smem_bytes(n_max, cap_near, cap_items) + ((size_t)4 * NM + 2 * (size_t)m + pk_canon_red_len(NM)) * 4;
 }
 
 extern "C" size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, int history)
@@ -436,9 +441,9 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
         return pk_fail(PK_EINVAL, "pk_relax: boundary / area terms need h%s");
     if (spec->pair_mode == PK_PAIR_LUT && !spec->lut.vals) return pk_fail(PK_EINVAL, "pk_relax: LUT without vals%s");
     const int T = pk_cost_threads(n_max);
-    // the item list must hold one full round (16 piece pairs per thread) beyond its flush level
-    const int cap = spec->pair_mode == PK_PAIR_LUT ? 4 * T : 20 * T;
-    const size_t smem = pk_relax_smem_bytes(n_max, cap, prm->history);
+    int cap_near, cap_items;
+    pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
+    const size_t smem = pk_relax_smem_bytes(n_max, cap_near, cap_items, prm->history);
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaSuccess;
     switch (spec->pair_mode) {
@@ -447,7 +452,7 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
         err = cudaFuncSetAttribute(pk_relax_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
         if (err == cudaSuccess)                                                                          \
             pk_relax_kernel<M><<<E, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, xyt_out, \
-                                                   h_out, loss_out, iters_out, work, cap);                \
+                                                   h_out, loss_out, iters_out, work, cap_near, cap_items); \
         break;
         PK_R(PK_PAIR_NONE)
         PK_R(PK_PAIR_AREA)
