@@ -199,6 +199,29 @@ int pk_relax(const float* xyt_in, const float* h_in, const int* offsets, const i
              const PkCostSpec* spec, const PkRelaxParams* params, float* xyt_out, float* h_out, float* loss_out,
              int* iters_out, float* work, void* stream);
 
+/* Allocation-free form of pk_relax for a uniform batch (E packings of n
+ * trees).  No counterpart in the reference: it exists for callers that must
+ * not allocate device memory while they run -- code inside CUDA stream
+ * capture, where cudaMalloc is not permitted; hosts whose allocator or memory
+ * budget owns every device byte; and latency-bound loops, where cudaMalloc /
+ * cudaFree may synchronise the device.  It allocates nothing: the L-BFGS
+ * history lives in a 16 MiB array built into the library, which every GPU
+ * that loads the library keeps until the process exits.  The caller still
+ * provides inputs and outputs as for pk_relax.
+ *   - Limit: 2 * history * E * (3 n + 3) <= 4194304 floats (e.g. E = 256,
+ *     n = 200, history = 10); larger batches return PK_ERANGE with a message.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - All calls share the one array and it keeps the previous call's
+ *     contents.  Nothing in it needs clearing (every history slot is written
+ *     before it is read), but two calls whose kernels overlap on the GPU --
+ *     on different streams, or from different host threads -- race on it:
+ *     serialise them. */
+int pk_relax_noalloc(const float* xyt_in, const float* h_in, int E, int n, const PkCostSpec* spec,
+                     const PkRelaxParams* params, float* xyt_out, float* h_out, float* loss_out, int* iters_out,
+                     void* stream);
+
 /* Floats of work needed by pk_relax: sizes_host (E,) host int32 tree counts
  * for a ragged batch, or NULL and n_uniform for a uniform one. */
 size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, int history);

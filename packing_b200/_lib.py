@@ -88,6 +88,8 @@ SIGNATURES = {
                  _P, _P, _P],
     "pk_relax_workspace_floats": [_P, _I, _I, _I],
     "pk_fma_probe": [_P, _I, _I, _I, _P],
+    "pk_relax_noalloc": [_P, _P, _I, _I, ctypes.POINTER(PkCostSpec), ctypes.POINTER(PkRelaxParams), _P, _P, _P, _P,
+                         _P],
 }
 RESTYPES = {"pk_last_error": ctypes.c_char_p, "pk_relax_workspace_floats": ctypes.c_size_t}
 

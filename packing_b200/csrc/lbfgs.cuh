@@ -464,3 +464,55 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
     if (err != cudaSuccess) return pk_cuda_check(err, "pk_relax attribute");
     return pk_cuda_check(cudaGetLastError(), "pk_relax launch");
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free relaxation: pk_relax with its L-BFGS history kept in a
+// fixed device array compiled into this library instead of a caller buffer.
+// The array is a file-scope __device__ symbol; host code may not use its name
+// as a pointer, so the device address is fetched once per device with
+// cudaGetSymbolAddress (on the first call made with that device current).
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#define PK_NOALLOC_HISTORY_FLOATS (4u * 1024u * 1024u)   // 16 MiB per device
+
+static __device__ __align__(256) float pk_noalloc_history[PK_NOALLOC_HISTORY_FLOATS];
+static float* g_pk_noalloc_ptr[64];
+static std::mutex g_pk_noalloc_mu;
+
+extern "C" int pk_relax_noalloc(const float* xyt_in, const float* h_in, int E, int n, const PkCostSpec* spec,
+                                const PkRelaxParams* params, float* xyt_out, float* h_out, float* loss_out,
+                                int* iters_out, void* stream)
+{
+    if (!params) return pk_fail(PK_EINVAL, "pk_relax_noalloc: params is NULL%s");
+    if (E < 0 || n < 0) return pk_fail(PK_EINVAL, "pk_relax_noalloc: negative size%s");
+    if (params->history < 1 || params->history > 64)
+        return pk_fail(PK_EINVAL, "pk_relax_noalloc: history must be in [1, 64]%s");
+    const unsigned long long need = 2ull * (unsigned long long)params->history * (unsigned long long)E *
+                                    (3ull * (unsigned long long)n + 3ull);
+    if (need > PK_NOALLOC_HISTORY_FLOATS) {
+        snprintf(g_pk_err, sizeof(g_pk_err),
+                 "pk_relax_noalloc: batch needs %llu history floats (2 * history * E * (3 n + 3)); the built-in "
+                 "array holds %u -- use pk_relax with a caller buffer or a smaller batch",
+                 need, (unsigned)PK_NOALLOC_HISTORY_FLOATS);
+        return PK_ERANGE;
+    }
+    int dev = 0;
+    int rc = pk_cuda_check(cudaGetDevice(&dev), "pk_relax_noalloc: cudaGetDevice");
+    if (rc) return rc;
+    if (dev < 0 || dev >= 64) return pk_fail(PK_ERANGE, "pk_relax_noalloc: device id beyond 63%s");
+    float* hist = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pk_noalloc_mu);
+        if (!g_pk_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            rc = pk_cuda_check(cudaGetSymbolAddress(&p, pk_noalloc_history),
+                               "pk_relax_noalloc: cudaGetSymbolAddress");
+            if (rc) return rc;
+            g_pk_noalloc_ptr[dev] = (float*)p;
+        }
+        hist = g_pk_noalloc_ptr[dev];
+    }
+    return pk_relax(xyt_in, h_in, nullptr, nullptr, E, n, spec, params, xyt_out, h_out, loss_out, iters_out, hist,
+                    stream);
+}
