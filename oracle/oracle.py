@@ -55,6 +55,7 @@ def lib():
         L.oracle_lut_cost.argtypes = [P, P, i, P, i, i, i, P, i, ctypes.c_double, P, P]
         L.oracle_hungarian.argtypes = [P, i, i, P, P, P]
         L.oracle_diversity_shortcut.argtypes = [P, P, i, i, i, ctypes.c_float, ctypes.c_float, i, P]
+        L.oracle_validate.argtypes = [P, i, i, P, P]
         L.oracle_num_threads.restype = i
         L.oracle_init(TREE_EXPANSION)
         _lib = L
@@ -144,6 +145,17 @@ def diversity_shortcut(pop, ref, cos_a, sin_a, mirror):
     lib().oracle_diversity_shortcut(_p(pop), _p(ref), Np, Nr, n, np.float32(cos_a), np.float32(sin_a),
                                     int(bool(mirror)), _p(out))
     return out.reshape(Np, Nr)
+
+
+def validate(xyt):
+    """FP64 legality (overlapping tree pairs) and bounding-square side of
+    each packing, ``pack_metric.py:127-147``.  xyt (E, n, 3)."""
+    xyt = np.ascontiguousarray(xyt, dtype=np.float64)
+    E, n, _ = xyt.shape
+    ov = np.zeros(E, dtype=np.int32)
+    side = np.zeros(E)
+    lib().oracle_validate(_p(xyt), E, n, _p(ov), _p(side))
+    return ov, side
 
 
 def compound_cost(xyt, h, w_boundary=1.0, w_overlap=1.0, use_separation=False, w_area=0.0,

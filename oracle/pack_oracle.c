@@ -35,6 +35,11 @@ static d2 g_tree[NTV];
 static double g_max_radius;
 static double g_cutoff_sq;
 static double g_tree_area;
+/* legality tree: the metric's unexpanded tree (pack_metric.py:27-79) in the
+ * search tree's pose frame (centroid offset of pack_io.py:150-158) */
+static d2 g_lpiece[MAXP][MAXV];
+static d2 g_ltree[NTV];
+static double g_lradius;
 
 static d2 mk(double x, double y) { d2 r; r.x = x; r.y = y; return r; }
 
@@ -96,6 +101,34 @@ void oracle_init(double E)
         if (r > g_max_radius) g_max_radius = r;
     }
     g_cutoff_sq = (2.0 * g_max_radius) * (2.0 * g_max_radius);
+    {
+        double lw = 0.15, lbw = 0.7, lmw = 0.4, ltw = 0.25, ltip = 0.8, lt1 = 0.5, lt2 = 0.25, lb = 0.0, lbot = -0.2;
+        d2 lpoly[NTV] = {
+            mk(0.0, ltip), mk(ltw / 2, lt1), mk(ltw / 4, lt1), mk(lmw / 2, lt2), mk(lmw / 4, lt2),
+            mk(lbw / 2, lb), mk(lw / 2, lb), mk(lw / 2, lbot), mk(-(lw / 2), lbot), mk(-(lw / 2), lb),
+            mk(-(lbw / 2), lb), mk(-(lmw / 4), lt2), mk(-(lmw / 2), lt2), mk(-(ltw / 4), lt1), mk(-(ltw / 2), lt1)};
+        d2 lpc[MAXP][MAXV] = {
+            {mk(0.0, ltip), mk(ltw / 2, lt1), mk(-(ltw / 2), lt1), mk(0, 0)},
+            {mk(ltw / 4, lt1), mk(lmw / 2, lt2), mk(-lmw / 2, lt2), mk(-ltw / 4, lt1)},
+            {mk(lmw / 4, lt2), mk(lbw / 2, lb), mk(-lbw / 2, lb), mk(-lmw / 4, lt2)},
+            {mk(lw / 2, lb), mk(lw / 2, lbot), mk(-lw / 2, lbot), mk(-lw / 2, lb)}};
+        g_lradius = 0.0;
+        for (int i = 0; i < NTV; ++i) {
+            g_ltree[i] = mk(lpoly[i].x - cx, lpoly[i].y - cy);
+            double r = sqrt(g_ltree[i].x * g_ltree[i].x + g_ltree[i].y * g_ltree[i].y);
+            if (r > g_lradius) g_lradius = r;
+        }
+        for (int p = 0; p < MAXP; ++p) {
+            d2 tmp[MAXV];
+            for (int v = 0; v < nv[p]; ++v) tmp[v] = mk(lpc[p][v].x - cx, lpc[p][v].y - cy);
+            if (signed_area(tmp, nv[p]) < 0.0) {
+                g_lpiece[p][0] = tmp[0];
+                for (int v = 1; v < nv[p]; ++v) g_lpiece[p][v] = tmp[nv[p] - v];
+            } else {
+                for (int v = 0; v < nv[p]; ++v) g_lpiece[p][v] = tmp[v];
+            }
+        }
+    }
     for (int p = 0; p < MAXP; ++p) {
         d2 tmp[MAXV];
         for (int v = 0; v < nv[p]; ++v) tmp[v] = mk(pc[p][v].x - cx, pc[p][v].y - cy);
@@ -660,6 +693,55 @@ void oracle_diversity_shortcut(const float* pop, const float* ref, int Np, int N
         }
         out[b] = tot;
         free(rx);
+    }
+}
+
+/* Legality and bounding square of E packings (pack_metric.score,
+ * pack_metric.py:127-147): overlaps[e] = tree pairs whose interiors meet
+ * (intersection area of some piece pair above 1e-14, computed by the
+ * Sutherland-Hodgman clip of pack_cuda_primitives.py:348-538 in double),
+ * side[e] = max(width, height) of the bounding box of all legality trees. */
+void oracle_validate(const double* xyt, int E, int n, int* overlaps, double* side)
+{
+    double cut = 4.0 * g_lradius * g_lradius * (1.0 + 1e-12);
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int e = 0; e < E; ++e) {
+        const double* X = xyt + (size_t)e * n * 3;
+        double bx0 = 1e300, bx1 = -1e300, by0 = 1e300, by1 = -1e300;
+        for (int t = 0; t < n; ++t) {
+            double c = cos(X[3 * t + 2]), s = sin(X[3 * t + 2]);
+            for (int v = 0; v < NTV; ++v) {
+                double vx = c * g_ltree[v].x - s * g_ltree[v].y + X[3 * t];
+                double vy = s * g_ltree[v].x + c * g_ltree[v].y + X[3 * t + 1];
+                bx0 = fmin(bx0, vx); bx1 = fmax(bx1, vx); by0 = fmin(by0, vy); by1 = fmax(by1, vy);
+            }
+        }
+        int cnt = 0;
+        for (int i = 0; i < n; ++i) {
+            for (int j = i + 1; j < n; ++j) {
+                double dx = X[3 * j] - X[3 * i], dy = X[3 * j + 1] - X[3 * i + 1];
+                if (dx * dx + dy * dy > cut) continue;
+                double ci = cos(X[3 * i + 2]), si = sin(X[3 * i + 2]);
+                double cj = cos(X[3 * j + 2]), sj = sin(X[3 * j + 2]);
+                int ov = 0;
+                for (int p = 0; p < MAXP && !ov; ++p) {
+                    d2 P[MAXV];
+                    for (int v = 0; v < g_piece_nv[p]; ++v)
+                        P[v] = mk(ci * g_lpiece[p][v].x - si * g_lpiece[p][v].y + X[3 * i],
+                                  si * g_lpiece[p][v].x + ci * g_lpiece[p][v].y + X[3 * i + 1]);
+                    for (int q = 0; q < MAXP && !ov; ++q) {
+                        d2 Q[MAXV];
+                        for (int v = 0; v < g_piece_nv[q]; ++v)
+                            Q[v] = mk(cj * g_lpiece[q][v].x - sj * g_lpiece[q][v].y + X[3 * j],
+                                      sj * g_lpiece[q][v].x + cj * g_lpiece[q][v].y + X[3 * j + 1]);
+                        if (convex_isect_area(P, g_piece_nv[p], Q, g_piece_nv[q], NULL) > 1e-14) ov = 1;
+                    }
+                }
+                cnt += ov;
+            }
+        }
+        overlaps[e] = cnt;
+        side[e] = n > 0 ? fmax(bx1 - bx0, by1 - by0) : 0.0;
     }
 }
 

@@ -31,6 +31,9 @@ class PkGeometry(ctypes.Structure):
         ("n_tree_verts", ctypes.c_int),
         ("max_radius", ctypes.c_double),
         ("area", ctypes.c_double),
+        ("has_legal", ctypes.c_int),
+        ("legal_piece_xy", ctypes.c_double * 2 * 4 * 4),
+        ("legal_tree_xy", ctypes.c_double * 2 * 16),
     ]
 
 
@@ -88,6 +91,7 @@ SIGNATURES = {
                  _P, _P, _P],
     "pk_relax_workspace_floats": [_P, _I, _I, _I],
     "pk_fma_probe": [_P, _I, _I, _I, _P],
+    "pk_validate_fp64": [_P, _I, _I, _I, _P, _P, _P],
     "pk_relax_noalloc": [_P, _P, _I, _I, ctypes.POINTER(PkCostSpec), ctypes.POINTER(PkRelaxParams), _P, _P, _P, _P,
                          _P],
 }

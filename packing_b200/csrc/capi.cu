@@ -7,6 +7,7 @@
 #include "cost.cuh"
 #include "lap.cuh"
 #include "lbfgs.cuh"
+#include "validate.cuh"
 
 extern "C" int pk_version(void) { return 1; }
 

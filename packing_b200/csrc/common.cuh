@@ -26,13 +26,17 @@ struct PkDevGeom {
     float coll_tiny;    // 2e-6 * longest piece edge: bound on |cross| of near-collinear points
 };
 
-// FP64 copy for the legality validator.
+// FP64 tables: the search tree, and the legality tree of the validator
+// (CCW pieces padded like the FP32 ones).
 struct PkDevGeom64 {
     double2 piece[PK_NUM_PIECES][4];
     int piece_nv[PK_NUM_PIECES];
     double2 tree[PK_MAX_TREE_VERTS];
     int n_tree;
     double max_radius;
+    double2 legal_piece[PK_NUM_PIECES][4];
+    double2 legal_tree[PK_MAX_TREE_VERTS];
+    double legal_radius;
 };
 
 __constant__ PkDevGeom c_geom;

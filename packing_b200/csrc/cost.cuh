@@ -125,41 +125,50 @@ __device__ __forceinline__ void pk_side_values(const float2 (&X)[4], const float
         for (int v = 0; v < 4; ++v) f[k][v] = pk_cross3_rn(Y[k], Y[(k + 1) & 3], X[v]);
 }
 
-// Some edge line of Y has every vertex of X strictly outside: X and Y are
-// disjoint (separating axis), no boundary portion of either lies in the other.
-__device__ __forceinline__ bool pk_separated(const float (&f)[4][4], bool y_tri)
-{
-    bool sep = false;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        if (k == 3 && y_tri) continue;
-        sep = sep || (f[k][0] < 0.f && f[k][1] < 0.f && f[k][2] < 0.f && f[k][3] < 0.f);
-    }
-    return sep;
-}
-
 // One pass of the assembly: the portions of X's edges inside Y, added to A2
 // (twice the area) and to g (gradient of X's rigid pose about centre ctr).
-// f holds X's vertices against Y's lines.  KEEP_SAME_DIR: a collinear edge
-// of X is kept when it runs the same way as Y's (X = Q) or always dropped
-// (X = P).  Crossing parameters use the fast divide (relative error a few
-// ulp); the sign logic is branch-free so lanes stay converged.
+// f holds X's vertices against Y's lines.  Per vertex, a 4-bit mask of the
+// lines it is outside of decides most edges without arithmetic: an edge
+// with both ends outside one line is empty, an edge with neither end
+// outside any line is whole, and only the lines it crosses get a crossing
+// parameter.  Returns false when some line of Y has every vertex of X
+// outside (separating axis: the pieces are disjoint).  KEEP_SAME_DIR: a
+// collinear edge of X is kept when it runs the same way as Y's (X = Q) or
+// always dropped (X = P).
 template <bool KEEP_SAME_DIR>
-__device__ __forceinline__ void pk_clip_pass(const float2 (&X)[4], bool x_tri, const float2 (&Y)[4], bool y_tri,
+__device__ __forceinline__ bool pk_clip_pass(const float2 (&X)[4], bool x_tri, const float2 (&Y)[4], bool y_tri,
                                              const float (&f)[4][4], float2 ctr, float& A2, float3& g)
 {
     const float tiny = c_geom.coll_tiny;
+    const unsigned lines = y_tri ? 0x7u : 0xFu;
+    unsigned out[4], nearm[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        unsigned o = 0, nm = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            o |= (unsigned)(f[k][v] < 0.f) << k;
+            nm |= (unsigned)(fabsf(f[k][v]) <= tiny) << k;
+        }
+        out[v] = o & lines;
+        nearm[v] = nm & lines;
+    }
+    if (out[0] & out[1] & out[2] & out[3]) return false;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
         if (v == 3 && x_tri) break;
-        const float2 a = X[v], b = X[(v + 1) & 3];
-        float tin = 0.f, tout = 1.f;
+        const int vb = (v + 1) & 3;
+        const float2 a = X[v], b = X[vb];
+        unsigned skip = 0;
         bool empty = false;
+        const unsigned coll = nearm[v] & nearm[vb];
+        if (coll) {
+            // both ends within tolerance of some line of Y: confirm collinearity
+            // with the symmetric four-number test (the other pass sees the same numbers)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (k == 3 && y_tri) continue;
-            const float fa = f[k][v], fb = f[k][(v + 1) & 3];
-            if (fabsf(fa) <= tiny && fabsf(fb) <= tiny) {
+            for (int k = 0; k < 4; ++k) {
+                if (!((coll >> k) & 1u)) continue;
+                const float fa = f[k][v], fb = f[k][vb];
                 const float2 ya = Y[k], yb = Y[(k + 1) & 3];
                 const float2 ey = make_float2(yb.x - ya.x, yb.y - ya.y), ex = make_float2(b.x - a.x, b.y - a.y);
                 const float ty = PK_COLLINEAR_TOL2 * __fmaf_rn(ey.x, ey.x, __fmul_rn(ey.y, ey.y));
@@ -167,16 +176,24 @@ __device__ __forceinline__ void pk_clip_pass(const float2 (&X)[4], bool x_tri, c
                 const float ra = pk_cross3_rn(a, b, ya), rb = pk_cross3_rn(a, b, yb);
                 if (fa * fa <= ty && fb * fb <= ty && ra * ra <= tx && rb * rb <= tx) {
                     if (!KEEP_SAME_DIR || ex.x * ey.x + ex.y * ey.y <= 0.f) empty = true;
-                    continue;
+                    skip |= 1u << k;
                 }
             }
-            const bool ia = fa >= 0.f, ib = fb >= 0.f;
-            const float t = __fdividef(fa, fa - fb);
-            empty = empty || (!ia && !ib);
-            tout = (ia && !ib) ? fminf(tout, t) : tout;
-            tin = (!ia && ib) ? fmaxf(tin, t) : tin;
         }
-        if (!empty && tin < tout) {
+        const unsigned oa = out[v] & ~skip, ob = out[vb] & ~skip;
+        if (empty || (oa & ob)) continue;
+        const unsigned crossm = oa | ob;
+        float tin = 0.f, tout = 1.f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if ((crossm >> k) & 1u) {
+                const float fa = f[k][v], fb = f[k][vb];
+                const float t = __fdividef(fa, fa - fb);
+                if ((oa >> k) & 1u) tin = fmaxf(tin, t);    // entering
+                else tout = fminf(tout, t);                 // leaving
+            }
+        }
+        if (tin < tout) {
             const float dt = tout - tin;
             const float2 e = make_float2(b.x - a.x, b.y - a.y);
             A2 += dt * pk_cross(a, b);
@@ -188,6 +205,7 @@ __device__ __forceinline__ void pk_clip_pass(const float2 (&X)[4], bool x_tri, c
             g.z += pk_cross(m, N);
         }
     }
+    return true;
 }
 
 __device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_tri,
@@ -200,14 +218,12 @@ __device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_
     area = 0.f;
     float f[4][4];
     pk_side_values(P, Q, f);
-    if (pk_separated(f, q_tri)) return;
-    pk_clip_pass<false>(P, p_tri, Q, q_tri, f, make_float2(0.f, 0.f), A2, gP);
+    if (!pk_clip_pass<false>(P, p_tri, Q, q_tri, f, make_float2(0.f, 0.f), A2, gP)) return;
     pk_side_values(Q, P, f);
-    if (pk_separated(f, p_tri)) {
+    if (!pk_clip_pass<true>(Q, q_tri, P, p_tri, f, d, A2, gQ)) {
         gP = make_float3(0.f, 0.f, 0.f);
         return;
     }
-    pk_clip_pass<true>(Q, q_tri, P, p_tri, f, d, A2, gQ);
     area = 0.5f * A2;
     if (!(area > 0.f)) {   // empty or numerically vanishing overlap
         area = 0.f;

@@ -1,0 +1,130 @@
+// validate.cuh -- strict FP64 legality and bounding-square side.
+//
+// The reference accepts a packing when no two trees have intersecting
+// interiors (shapely intersects and not touches at 1e18 scale,
+// pack_metric.py:127-141) and scores the side of the bounding square
+// (:144-147).  Here, per packing, one CTA checks every pair of trees within
+// twice the legality tree's radius piece by piece: two convex pieces have
+// disjoint interiors iff one of their edge normals separates them with a gap
+// >= 0 (separating-axis test, exact comparisons in double), so touching is
+// legal as in the metric.
+#pragma once
+#include "common.cuh"
+
+__device__ __forceinline__ bool pk_pieces_overlap64(const double2 (&P)[4], bool pt, const double2 (&Q)[4], bool qt)
+{
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool tri = pass == 0 ? pt : qt;
+            if (k == 3 && tri) continue;
+            const double2 a = pass == 0 ? P[k] : Q[k];
+            const double2 b = pass == 0 ? P[(k + 1) & 3] : Q[(k + 1) & 3];
+            const double nx = -(b.y - a.y), ny = b.x - a.x;
+            double mn1 = 1e300, mx1 = -1e300, mn2 = 1e300, mx2 = -1e300;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const double p1 = __dmul_rn(P[v].x, nx) + __dmul_rn(P[v].y, ny);
+                const double p2 = __dmul_rn(Q[v].x, nx) + __dmul_rn(Q[v].y, ny);
+                mn1 = fmin(mn1, p1); mx1 = fmax(mx1, p1);
+                mn2 = fmin(mn2, p2); mx2 = fmax(mx2, p2);
+            }
+            if (mx1 <= mn2 || mx2 <= mn1) return false;   // separating axis (touching allowed)
+        }
+    }
+    return true;
+}
+
+template <typename T>
+__global__ void pk_validate_kernel(const T* __restrict__ xyt, int E, int n, int* __restrict__ overlaps,
+                                   double* __restrict__ side)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    double4* pose = (double4*)pk_smem;            // x, y, cos, sin
+    double* red = (double*)(pose + n);            // 32
+    int* redi = (int*)(red + 32);                 // 32
+    const int e = blockIdx.x;
+    if (e >= E) return;
+    const T* X = xyt + (size_t)e * n * 3;
+    double bx0 = 1e300, bx1 = -1e300, by0 = 1e300, by1 = -1e300;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const double x = (double)X[3 * t], y = (double)X[3 * t + 1], th = (double)X[3 * t + 2];
+        double s, c;
+        sincos(th, &s, &c);
+        pose[t] = make_double4(x, y, c, s);
+        for (int v = 0; v < c_geom64.n_tree; ++v) {
+            const double2 l = c_geom64.legal_tree[v];
+            const double vx = c * l.x - s * l.y + x, vy = s * l.x + c * l.y + y;
+            bx0 = fmin(bx0, vx); bx1 = fmax(bx1, vx);
+            by0 = fmin(by0, vy); by1 = fmax(by1, vy);
+        }
+    }
+    bx0 = -pk_block_max<double>(-bx0, red);
+    bx1 = pk_block_max<double>(bx1, red);
+    by0 = -pk_block_max<double>(-by0, red);
+    by1 = pk_block_max<double>(by1, red);
+    const double cut = 4.0 * c_geom64.legal_radius * c_geom64.legal_radius * (1.0 + 1e-12);
+    int count = 0;
+    const long long npairs = (long long)n * (n - 1) / 2;
+    for (long long k = threadIdx.x; k < npairs; k += blockDim.x) {
+        const int dd = (int)(k / n);
+        const int i = (int)(k - (long long)dd * n);
+        int j = i + dd + 1;
+        if (j >= n) j -= n;
+        const double4 A = pose[i], B = pose[j];
+        const double dx = B.x - A.x, dy = B.y - A.y;
+        if (dx * dx + dy * dy > cut) continue;
+        bool ov = false;
+        for (int p = 0; p < 4 && !ov; ++p) {
+            double2 P[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const double2 l = c_geom64.legal_piece[p][v];
+                P[v] = make_double2(A.z * l.x - A.w * l.y + A.x, A.w * l.x + A.z * l.y + A.y);
+            }
+            for (int q = 0; q < 4 && !ov; ++q) {
+                double2 Q[4];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const double2 l = c_geom64.legal_piece[q][v];
+                    Q[v] = make_double2(B.z * l.x - B.w * l.y + B.x, B.w * l.x + B.z * l.y + B.y);
+                }
+                ov = pk_pieces_overlap64(P, c_geom64.piece_nv[p] == 3, Q, c_geom64.piece_nv[q] == 3);
+            }
+        }
+        count += ov ? 1 : 0;
+    }
+    count = pk_block_sum<int>(count, redi);
+    if (threadIdx.x == 0) {
+        overlaps[e] = count;
+        side[e] = n > 0 ? fmax(bx1 - bx0, by1 - by0) : 0.0;
+    }
+}
+
+extern "C" int pk_validate_fp64(const void* xyt, int dtype_bytes, int E, int n, int* overlaps, double* side,
+                                void* stream)
+{
+    int rc = pk_check_init();
+    if (rc) return rc;
+    if (E < 0 || n < 0) return pk_fail(PK_EINVAL, "pk_validate_fp64: negative size%s");
+    if (n > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_validate_fp64: more than 1024 trees%s");
+    if (E == 0) return PK_OK;
+    if ((!xyt && n > 0) || !overlaps || !side) return pk_fail(PK_EINVAL, "pk_validate_fp64: NULL pointer%s");
+    const int T = n <= 64 ? 64 : (n <= 128 ? 128 : 256);
+    const size_t smem = (size_t)n * 32 + 32 * 8 + 32 * 4;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t err;
+    if (dtype_bytes == 4) {
+        err = cudaFuncSetAttribute(pk_validate_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err == cudaSuccess) pk_validate_kernel<float><<<E, T, smem, st>>>((const float*)xyt, E, n, overlaps, side);
+    } else if (dtype_bytes == 8) {
+        err = cudaFuncSetAttribute(pk_validate_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err == cudaSuccess)
+            pk_validate_kernel<double><<<E, T, smem, st>>>((const double*)xyt, E, n, overlaps, side);
+    } else {
+        return pk_fail(PK_EINVAL, "pk_validate_fp64: dtype must be float32 or float64%s");
+    }
+    if (err != cudaSuccess) return pk_cuda_check(err, "pk_validate_fp64 attribute");
+    return pk_cuda_check(cudaGetLastError(), "pk_validate_fp64 launch");
+}
