@@ -216,6 +216,38 @@ int pk_relax(const float* xyt_in, const float* h_in, const int* offsets, const i
              const PkCostSpec* spec, const PkRelaxParams* params, float* xyt_out, float* h_out, float* loss_out,
              int* iters_out, float* work, void* stream);
 
+/* ---- serving: resumable device-resident relaxation jobs ---------------- */
+
+#define PK_JOB_NEW 0
+#define PK_JOB_RUNNING 1
+#define PK_JOB_DONE 2
+
+/* One relaxation job of the serving loop.  Its state lives in a caller pool:
+ * pool[x_off ..] = x (3n + 3: xyt then h), g (3n + 3), ro (history);
+ * pool[h_off ..] = S, Y (2 * history * (3n + 3)).  The caller writes x and
+ * sets status = PK_JOB_NEW; the library fills the rest. */
+typedef struct PkJob {
+    int n;
+    int max_iter;
+    long long x_off;
+    long long h_off;
+    int status;
+    int it, evals, hlen, hstart;
+    float H, loss, loss0;
+} PkJob;
+
+/* Advances every job listed (device int32 indices into jobs, largest n
+ * first balances the launch) by up to chunk_iters L-BFGS iterations of the
+ * compound cost *spec; params->history and the step / tolerance settings
+ * apply to all jobs, each job's own max_iter to itself; the final loss is
+ * evaluated at the returned x.  A job's result does not depend on which
+ * jobs share its launches or on how its iterations are split into chunks.
+ * The continuous-batching form of pack_dynamics.run_simulation_list
+ * (pack_dynamics.py:152-236), which runs one blocking relaxation per tree
+ * count. */
+int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* pool, int n_max, const PkCostSpec* spec,
+                  const PkRelaxParams* params, int chunk_iters, void* stream);
+
 /* Allocation-free form of pk_relax for a uniform batch (E packings of n
  * trees).  No counterpart in the reference: it exists for callers that must
  * not allocate device memory while they run -- code inside CUDA stream

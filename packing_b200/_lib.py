@@ -69,6 +69,19 @@ class PkRelaxParams(ctypes.Structure):
     ]
 
 
+class PkJob(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int), ("max_iter", ctypes.c_int),
+        ("x_off", ctypes.c_longlong), ("h_off", ctypes.c_longlong),
+        ("status", ctypes.c_int), ("it", ctypes.c_int), ("evals", ctypes.c_int),
+        ("hlen", ctypes.c_int), ("hstart", ctypes.c_int),
+        ("H", ctypes.c_float), ("loss", ctypes.c_float), ("loss0", ctypes.c_float),
+    ]
+
+
+PK_JOB_NEW, PK_JOB_RUNNING, PK_JOB_DONE = 0, 1, 2
+
+
 # (name, argtypes) of every exported entry point; include/packb200.h is the
 # authoritative declaration.
 _P, _I, _F, _D = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double
@@ -92,6 +105,7 @@ SIGNATURES = {
     "pk_relax_workspace_floats": [_P, _I, _I, _I],
     "pk_fma_probe": [_P, _I, _I, _I, _P],
     "pk_validate_fp64": [_P, _I, _I, _I, _P, _P, _P],
+    "pk_relax_jobs": [_P, _P, _I, _P, _I, ctypes.POINTER(PkCostSpec), ctypes.POINTER(PkRelaxParams), _I, _P],
     "pk_relax_noalloc": [_P, _P, _I, _I, ctypes.POINTER(PkCostSpec), ctypes.POINTER(PkRelaxParams), _P, _P, _P, _P,
                          _P],
 }

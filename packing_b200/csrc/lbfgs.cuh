@@ -268,14 +268,122 @@ extern "C" int pk_lbfgs_phase(int phase, int dtype_bytes, void* const* arrays, i
 }
 
 // ---------------------------------------------------------------------------
-// Fused relaxation: one CTA per packing runs the whole L-BFGS loop with the
+// Fused relaxation: one CTA per packing runs the L-BFGS loop with the
 // compound cost evaluated in place.  x = [xyt (3n), h (3)] as in
 // pack_dynamics.py:76-83.  Per-instance stop: an instance that becomes
 // inactive stops stepping (the reference keeps stepping inactive systems
 // while another system of the same batch is still active, so with this form
 // an instance's result never depends on the rest of the batch).  The cost is
-// evaluated at one place in the loop (smaller code than one copy per use).
+// evaluated at one place in the loop.
 // ---------------------------------------------------------------------------
+struct PkRelaxVars {
+    int it, evals, hlen, hstart, active;
+    float H, loss, loss0, ploss, t;
+};
+
+// Runs iterations until the relaxation finishes (returns true) or, after the
+// history update of iteration it_stop, pauses (returns false) with x, g, the
+// history and v complete, so a later call with resume = true continues
+// exactly where this one stopped.  resume = false starts from x (evaluates
+// it first).  All threads of the block call it.
+template <int MODE>
+__device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float* al, float* ro, float* red, int& flip,
+                                 float* S, float* Y, int n, bool use_h, const PkCostSpec& spec,
+                                 const PkRelaxParams& prm, const PkCostSmem& sm, PkRelaxVars& v, bool resume,
+                                 int it_stop, unsigned long long& hist_streamed)
+{
+    const int N = 3 * n + 3;
+    const int m = prm.history;
+    bool need_eval = !resume, final_pending = false, want_grad = true, skip_update = resume;
+    for (;;) {
+        if (need_eval) {
+            __syncthreads();   // x complete
+            const double L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, want_grad ? g : nullptr,
+                                                    (want_grad && use_h) ? g + 3 * n : nullptr, sm);
+            v.loss = (float)L;
+        }
+        if (final_pending) return true;
+        if (!skip_update) {
+            if (v.it == 0) {
+                // initial point (:489-500)
+                v.loss0 = v.loss;
+                const float gm = pk_own_absmax<float>(N, g, 1.f, red);
+                v.active = !(gm <= prm.tol_grad);
+            } else {
+                // after a step (:632-724)
+                ++v.evals;
+                if (v.it > 1) {
+                    const float t = v.t;
+                    const float ys =
+                        pk_canon_sum<float>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red, flip);
+                    const float yy = pk_canon_sum<float>(
+                        N, [&](int k) { const float y = g[k] - pg[k]; return y * y; }, red, flip);
+                    if (ys > 1e-10f) {
+                        int slot;
+                        if (v.hlen < m) { slot = (v.hstart + v.hlen) % m; ++v.hlen; }
+                        else { slot = v.hstart; v.hstart = (v.hstart + 1) % m; }
+                        float* Sd = S + (size_t)slot * N;
+                        float* Yd = Y + (size_t)slot * N;
+                        PK_OWN_LOOP(k, N) {
+                            Yd[k] = g[k] - pg[k];
+                            Sd[k] = d[k] * t;
+                        }
+                        v.H = ys / yy;
+                        if (threadIdx.x == 0) ro[slot] = 1.f / ys;
+                    }
+                }
+                const float gmax = pk_own_absmax<float>(N, g, 1.f, red);
+                const float pc = pk_own_absmax<float>(N, d, v.t, red);
+                if (gmax <= prm.tol_grad) v.active = 0;
+                if (v.evals >= prm.max_eval) v.active = 0;
+                if (pc <= prm.tol_change) v.active = 0;
+                const float lc = fabsf(v.loss - v.ploss);
+                if (lc < prm.tol_change) v.active = 0;
+                if (prm.tol_rel_change > 0.f && v.it > m && lc / (fabsf(v.ploss) + 1e-12f) < prm.tol_rel_change)
+                    v.active = 0;
+                if (prm.stop_on_cost_increase && v.loss > v.loss0) v.active = 0;
+            }
+        }
+        skip_update = false;
+        if (!v.active || v.it >= prm.max_iter) return true;
+        if (v.it >= it_stop) return false;
+        // ---- next step (:531-631) ----
+        ++v.it;
+        if (v.it == 1) {
+            PK_OWN_LOOP(k, N) d[k] = -g[k];
+            v.H = 1.f;
+        } else {
+            pk_two_loop<float>(g, d, N, S, Y, ro, m, v.hlen, v.hstart, v.H, al, red, flip);
+            hist_streamed += (unsigned long long)v.hlen;
+        }
+        PK_OWN_LOOP(k, N) pg[k] = g[k];
+        v.ploss = v.loss;
+        float t;
+        if (v.it == 1) {
+            const float gs = pk_canon_sum<float>(N, [&](int k) { return fabsf(g[k]); }, red, flip);
+            t = 1.f / gs;
+            t = (t < 1.f ? t : 1.f) * prm.lr;
+        } else {
+            t = prm.lr;
+        }
+        if (prm.has_max_step) {
+            const float pc = pk_own_absmax<float>(N, d, t, red);
+            if (pc > prm.max_step) t = t * (prm.max_step / pc);
+        }
+        v.t = t;
+        const float gtd = pk_canon_sum<float>(N, [&](int k) { return g[k] * d[k]; }, red, flip);
+        if (gtd > -prm.tol_change) { v.active = 0; --v.it; return true; }
+        PK_OWN_LOOP(k, N) x[k] = x[k] + t * d[k];
+        need_eval = v.it != prm.max_iter;
+        if (!need_eval && prm.final_eval) {
+            // the last step is not evaluated by the reference loop; evaluate once for the final loss
+            need_eval = true;
+            want_grad = false;
+            final_pending = true;
+        }
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in,
                                 const int* __restrict__ offsets, const int* __restrict__ order, int E, int n_max,
@@ -311,100 +419,89 @@ __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restric
     for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) x[k] = xyt_in[(size_t)base * 3 + k];
     if (threadIdx.x < 3) x[3 * n + threadIdx.x] = h_in ? h_in[3 * e + threadIdx.x] : 0.f;
     if (threadIdx.x < 3) g[3 * n + threadIdx.x] = 0.f;
-    const bool use_h = h_in != nullptr;
-    float loss = 0.f, loss0 = 0.f, ploss = 0.f, H = 1.f, t = 0.f;
-    int evals = 1, hlen = 0, hstart = 0, it = 0;
+    PkRelaxVars v;
+    v.it = 0; v.evals = 1; v.hlen = 0; v.hstart = 0; v.active = 1;
+    v.H = 1.f; v.loss = 0.f; v.loss0 = 0.f; v.ploss = 0.f; v.t = 0.f;
     unsigned long long hist_streamed = 0;
-    bool active = true, need_eval = true, final_pending = false, want_grad = true;
-    for (;;) {
-        if (need_eval) {
-            __syncthreads();   // x complete
-            const double L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, want_grad ? g : nullptr,
-                                                    (want_grad && use_h) ? g + 3 * n : nullptr, sm);
-            loss = (float)L;
-        }
-        if (final_pending) break;
-        if (it == 0) {
-            // initial point (:489-500)
-            loss0 = loss;
-            const float gm = pk_own_absmax<float>(N, g, 1.f, red);
-            active = !(gm <= prm.tol_grad);
-        } else {
-            // after a step (:632-724)
-            ++evals;
-            if (it > 1) {
-                const float ys = pk_canon_sum<float>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red, flip);
-                const float yy = pk_canon_sum<float>(N, [&](int k) { const float y = g[k] - pg[k]; return y * y; },
-                                                     red, flip);
-                if (ys > 1e-10f) {
-                    int slot;
-                    if (hlen < m) { slot = (hstart + hlen) % m; ++hlen; }
-                    else { slot = hstart; hstart = (hstart + 1) % m; }
-                    float* Sd = S + (size_t)slot * N;
-                    float* Yd = Y + (size_t)slot * N;
-                    PK_OWN_LOOP(k, N) {
-                        Yd[k] = g[k] - pg[k];
-                        Sd[k] = d[k] * t;
-                    }
-                    H = ys / yy;
-                    if (threadIdx.x == 0) ro[slot] = 1.f / ys;
-                }
-            }
-            const float gmax = pk_own_absmax<float>(N, g, 1.f, red);
-            const float pc = pk_own_absmax<float>(N, d, t, red);
-            if (gmax <= prm.tol_grad) active = false;
-            if (evals >= prm.max_eval) active = false;
-            if (pc <= prm.tol_change) active = false;
-            const float lc = fabsf(loss - ploss);
-            if (lc < prm.tol_change) active = false;
-            if (prm.tol_rel_change > 0.f && it > m && lc / (fabsf(ploss) + 1e-12f) < prm.tol_rel_change) active = false;
-            if (prm.stop_on_cost_increase && loss > loss0) active = false;
-        }
-        if (!active || it >= prm.max_iter) break;
-        // ---- next step (:531-631) ----
-        ++it;
-        if (it == 1) {
-            PK_OWN_LOOP(k, N) d[k] = -g[k];
-            H = 1.f;
-        } else {
-            pk_two_loop<float>(g, d, N, S, Y, ro, m, hlen, hstart, H, al, red, flip);
-            hist_streamed += (unsigned long long)hlen;
-        }
-        PK_OWN_LOOP(k, N) pg[k] = g[k];
-        ploss = loss;
-        if (it == 1) {
-            const float gs = pk_canon_sum<float>(N, [&](int k) { return fabsf(g[k]); }, red, flip);
-            t = 1.f / gs;
-            t = (t < 1.f ? t : 1.f) * prm.lr;
-        } else {
-            t = prm.lr;
-        }
-        if (prm.has_max_step) {
-            const float pc = pk_own_absmax<float>(N, d, t, red);
-            if (pc > prm.max_step) t = t * (prm.max_step / pc);
-        }
-        const float gtd = pk_canon_sum<float>(N, [&](int k) { return g[k] * d[k]; }, red, flip);
-        if (gtd > -prm.tol_change) { active = false; --it; break; }
-        PK_OWN_LOOP(k, N) x[k] = x[k] + t * d[k];
-        need_eval = it != prm.max_iter;
-        if (!need_eval && prm.final_eval) {
-            // the last step is not evaluated by the reference loop; evaluate once for loss_out
-            need_eval = true;
-            want_grad = false;
-            final_pending = true;
-        }
-    }
+    pk_relax_iterate<MODE>(x, g, pg, d, al, ro, red, flip, S, Y, n, h_in != nullptr, spec, prm, sm, v, false,
+                           prm.max_iter, hist_streamed);
     __syncthreads();
     for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) xyt_out[(size_t)base * 3 + k] = x[k];
     if (h_out && threadIdx.x < 3) h_out[3 * e + threadIdx.x] = x[3 * n + threadIdx.x];
     if (threadIdx.x == 0) {
-        loss_out[e] = loss;
-        if (iters_out) iters_out[e] = it;
+        loss_out[e] = v.loss;
+        if (iters_out) iters_out[e] = v.it;
         if (prm.counters) {
             for (int k = 0; k < 4; ++k) atomicAdd(&prm.counters[k], (unsigned long long)sm.cnt[k]);
-            atomicAdd(&prm.counters[4], (unsigned long long)it);
+            atomicAdd(&prm.counters[4], (unsigned long long)v.it);
             atomicAdd(&prm.counters[5], hist_streamed * (unsigned long long)N);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Resumable relaxation of device-resident jobs (the serving loop's engine).
+// Each job keeps x = [xyt, h], its gradient, its L-BFGS history and scalars
+// in a device pool between launches; one launch advances every listed job by
+// up to chunk_iters iterations.  Because the pause point is the end of an
+// iteration and every reduction is order-fixed, a job's result is the same
+// whatever other jobs share its launches and however its iterations are
+// split into chunks.
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict__ jobs, const int* __restrict__ list,
+                                     int njobs, float* __restrict__ pool, int n_max, PkCostSpec spec,
+                                     PkRelaxParams prm, int chunk_iters, int cap_near, int cap_items)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    PkJob* J = &jobs[list[blockIdx.x]];
+    const int n = J->n;
+    if (J->status == PK_JOB_DONE || n < 0 || n > n_max) return;
+    const int N = 3 * n + 3;
+    const int NM = 3 * n_max + 3;
+    const int m = prm.history;
+    PkRelaxParams p = prm;
+    p.max_iter = J->max_iter;
+    p.max_eval = J->max_iter * 5 / 4;
+    p.final_eval = 1;
+    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap_near, cap_items);
+    if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
+    float* x = (float*)(pk_smem + pk_cost_smem_bytes(n_max, cap_near, cap_items));
+    float* g = x + NM;
+    float* pg = g + NM;
+    float* d = pg + NM;
+    float* al = d + NM;
+    float* ro = al + m;
+    float* red = ro + m;
+    int flip = 0;
+    float* gx = pool + J->x_off;        // x (N), g (N), ro (m)
+    float* S = pool + J->h_off;         // S (m N), Y (m N)
+    float* Y = S + (size_t)m * N;
+    const bool resume = J->status == PK_JOB_RUNNING;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        x[k] = gx[k];
+        if (resume) g[k] = gx[N + k];
+    }
+    if (threadIdx.x < m && resume) ro[threadIdx.x] = gx[2 * N + threadIdx.x];
+    if (threadIdx.x < 3 && !resume) g[3 * n + threadIdx.x] = 0.f;
+    PkRelaxVars v;
+    v.it = J->it; v.evals = J->evals; v.hlen = J->hlen; v.hstart = J->hstart; v.active = 1;
+    v.H = J->H; v.loss = J->loss; v.loss0 = J->loss0; v.ploss = 0.f; v.t = 0.f;
+    if (!resume) { v.it = 0; v.evals = 1; v.hlen = 0; v.hstart = 0; v.H = 1.f; }
+    unsigned long long hs = 0;
+    const int it_stop = min(p.max_iter, v.it + max(chunk_iters, 1));
+    const bool finished = pk_relax_iterate<MODE>(x, g, pg, d, al, ro, red, flip, S, Y, n, true, spec, p, sm, v,
+                                                 resume, it_stop, hs);
+    __syncthreads();
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        gx[k] = x[k];
+        gx[N + k] = g[k];
+    }
+    if (threadIdx.x < m) gx[2 * N + threadIdx.x] = ro[threadIdx.x];
+    if (threadIdx.x == 0) {
+        J->it = v.it; J->evals = v.evals; J->hlen = v.hlen; J->hstart = v.hstart;
+        J->H = v.H; J->loss = v.loss; J->loss0 = v.loss0;
+        J->status = finished ? PK_JOB_DONE : PK_JOB_RUNNING;
     }
 }
 
@@ -463,6 +560,43 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
     }
     if (err != cudaSuccess) return pk_cuda_check(err, "pk_relax attribute");
     return pk_cuda_check(cudaGetLastError(), "pk_relax launch");
+}
+
+extern "C" int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* pool, int n_max, const PkCostSpec* spec,
+                             const PkRelaxParams* prm, int chunk_iters, void* stream)
+{
+    int rc = pk_check_init();
+    if (rc) return rc;
+    if (!spec || !prm) return pk_fail(PK_EINVAL, "pk_relax_jobs: spec and params are required%s");
+    if (njobs < 0 || n_max < 0) return pk_fail(PK_EINVAL, "pk_relax_jobs: negative size%s");
+    if (njobs == 0) return PK_OK;
+    if (n_max > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_relax_jobs: more than 1024 trees per job%s");
+    if (prm->history < 1 || prm->history > 64) return pk_fail(PK_EINVAL, "pk_relax_jobs: history must be in [1, 64]%s");
+    if (!jobs || !list || !pool) return pk_fail(PK_EINVAL, "pk_relax_jobs: NULL pointer%s");
+    if (spec->pair_mode == PK_PAIR_LUT && !spec->lut.vals) return pk_fail(PK_EINVAL, "pk_relax_jobs: LUT without vals%s");
+    const int T = pk_cost_threads(n_max);
+    int cap_near, cap_items;
+    pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
+    const size_t smem = pk_relax_smem_bytes(n_max, cap_near, cap_items, prm->history);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t err = cudaSuccess;
+    switch (spec->pair_mode) {
+#define PK_J(M)                                                                                          \
+    case M:                                                                                              \
+        err = cudaFuncSetAttribute(pk_relax_jobs_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        if (err == cudaSuccess)                                                                          \
+            pk_relax_jobs_kernel<M><<<njobs, T, smem, st>>>(jobs, list, njobs, pool, n_max, *spec, *prm, chunk_iters, \
+                                                            cap_near, cap_items);                        \
+        break;
+        PK_J(PK_PAIR_NONE)
+        PK_J(PK_PAIR_AREA)
+        PK_J(PK_PAIR_SEP)
+        PK_J(PK_PAIR_LUT)
+#undef PK_J
+        default: return pk_fail(PK_EINVAL, "pk_relax_jobs: unknown pair_mode%s");
+    }
+    if (err != cudaSuccess) return pk_cuda_check(err, "pk_relax_jobs attribute");
+    return pk_cuda_check(cudaGetLastError(), "pk_relax_jobs launch");
 }
 
 // ---------------------------------------------------------------------------
