@@ -287,6 +287,14 @@ def run_ours(args, rank, world, dev):
                                        "host loop) over packing_b200.cost.compound_cost",
                                "fused_over_plain": value / (Ep / pt)}
 
+    # ---- secondary configurations: serving, ragged LUT, GA generation ----
+    if not args.skip_extra:
+        for name, fn in [("serve", measure_serve), ("ragged_lut", measure_ragged_lut), ("ga_step", measure_ga_step)]:
+            try:
+                out[name] = fn(args, dev)
+            except Exception as exc:   # reported, the headline stands
+                out[name] = {"error": f"{type(exc).__name__}: {exc}"}
+
     # ---- CPU baseline (oracle, host cores) ----
     if not args.skip_cpu:
         v, cores, dt = cpu_baseline_relax(args.cpu_E, n, iters, hist)
@@ -294,6 +302,182 @@ def run_ours(args, rank, world, dev):
                                "sample": f"{args.cpu_E} packings x n={n}, {iters} iterations, m={hist} "
                                          f"({dt:.1f} s, FP64 C oracle + numpy lbfgs restatement)"}
     return out
+
+
+def _serve_requests(count, seed):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(10), np.log(200)))))
+        xyt, h = workload(1, n, seed=seed * 100003 + k)
+        reqs.append((xyt[0], h[0], int(rng.integers(50, 301))))
+    return reqs
+
+
+def measure_serve(args, dev):
+    """10,000 requests, n log-uniform in [10, 200], 50-300 iterations, Poisson
+    arrivals at ~80% of the measured service capacity; against the same jobs
+    run batch by batch through the plain drop-in (grouped by tree count as
+    pack_dynamics.run_simulation_list does)."""
+    import torch
+
+    from packing_b200.cost import CostSpec, compound_cost
+    from packing_b200.lbfgs_torch_parallel import lbfgs
+    from packing_b200.serve import RelaxServer
+    spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
+    hist = args.history
+    # capacity: a saturating burst
+    burst = _serve_requests(args.serve_burst, seed=7)
+    srv = RelaxServer(spec, history=hist, chunk_iters=args.serve_chunk, device=dev)
+    srv.run_trace(burst[:64], np.zeros(64))
+    srv = RelaxServer(spec, history=hist, chunk_iters=args.serve_chunk, device=dev)
+    cap, _ = srv.run_trace(burst, np.zeros(len(burst)))
+    capacity = cap["relaxations_per_s"]
+    # Poisson trace at 80 % of capacity
+    reqs = _serve_requests(args.serve_requests, seed=11)
+    rate = 0.8 * capacity
+    arrivals = np.cumsum(np.random.default_rng(12).exponential(1.0 / rate, size=len(reqs)))
+    srv = RelaxServer(spec, history=hist, chunk_iters=args.serve_chunk, device=dev)
+    stats, done = srv.run_trace(reqs, arrivals)
+    assert all(r.iterations == r.iters for r in done)
+    # batch-by-batch plain form on a subset: all requests available, batches
+    # of args.serve_plain_batch, one drop-in lbfgs per distinct tree count
+    sub = reqs[:args.serve_plain]
+    t0 = time.perf_counter()
+    for b0 in range(0, len(sub), args.serve_plain_batch):
+        batch = sub[b0:b0 + args.serve_plain_batch]
+        groups = {}
+        for xyt, h, it in batch:
+            groups.setdefault(xyt.shape[0], []).append((xyt, h, it))
+        for n, grp in groups.items():
+            E = len(grp)
+            it = max(g[2] for g in grp)
+            x0 = torch.from_numpy(np.stack([np.concatenate([g[0].reshape(-1), g[1]]) for g in grp])).to(dev)
+            cb = torch.empty(E, device=dev)
+            gb = torch.empty((E, n, 3), device=dev)
+            ghb = torch.empty((E, 3), device=dev)
+
+            def f(x, is_main, n=n, E=E, cb=cb, gb=gb, ghb=ghb):
+                compound_cost(x[:, :3 * n].reshape(E, n, 3).contiguous(), x[:, 3 * n:].contiguous(), spec,
+                              out_cost=cb, out_grad=gb, out_grad_h=ghb)
+                return cb, torch.cat([gb.reshape(E, -1), ghb], 1)
+
+            lbfgs(f, x0, max_iter=it, history_size=hist, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+            x0.cpu()
+    plain = len(sub) / (time.perf_counter() - t0)
+    return {"requests": stats["requests"], "arrival_rate_per_s": rate, "capacity_per_s": capacity,
+            "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"], "relaxations_per_s": stats["relaxations_per_s"],
+            "engine_launches": stats["launches"], "chunk_iters": args.serve_chunk,
+            "plain_batch_by_batch_per_s": plain, "plain_sample": f"first {len(sub)} requests, batches of "
+                                                                 f"{args.serve_plain_batch}, grouped by n",
+            "served_over_plain": stats["relaxations_per_s"] / plain,
+            "workload": "n log-uniform [10,200], iterations U{50..300}, Poisson arrivals at 0.8 x capacity, m="
+                        f"{hist}, max_step 0.01, boundary + overlap area"}
+
+
+def measure_ragged_lut(args, dev):
+    """8192 instances, n log-uniform in [5, 200], LUT 256 x 256 x 360 built
+    from the overlap-area kernel; one launch relaxes them all."""
+    import torch
+
+    from packing_b200 import pack_cuda_lut
+    from packing_b200.cost import CostSpec
+    from packing_b200.pack_cuda_lut import LookupTable
+    from packing_b200.relax import RelaxParams, relax_into, workspace_floats
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    X = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 510, dtype=np.float32)[254:]
+    Y = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 256, dtype=np.float32)
+    T = np.linspace(-np.pi, np.pi, 360, dtype=np.float32)
+    lut = LookupTable.build_from_kernel("area", X=X, Y=Y, theta=T, trim_zeros=False, device=dev)
+    torch.cuda.synchronize(dev)
+    build_s = time.perf_counter() - t0
+    rng = np.random.default_rng(5)
+    E = args.lut_E
+    sizes = np.round(np.exp(rng.uniform(np.log(5), np.log(200), size=E))).astype(int)
+    xs = [workload(1, int(nn), seed=1000 + k)[0][0] for k, nn in enumerate(sizes)]
+    hs = np.concatenate([workload(1, int(nn), seed=0)[1] for nn in sizes])
+    flat = torch.from_numpy(np.concatenate(xs)).to(dev)
+    off = torch.tensor(np.concatenate([[0], np.cumsum(sizes)]), dtype=torch.int32, device=dev)
+    order = torch.tensor(np.argsort(-sizes, kind="stable"), dtype=torch.int32, device=dev)
+    h = torch.from_numpy(hs).to(dev)
+    spec = CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=0.0, fixed_h=True, lut=lut)
+    prm = RelaxParams(n_iterations=args.iters, history_size=args.history, max_step=0.01, final_eval=False)
+    xo = torch.empty_like(flat)
+    ho = torch.empty_like(h)
+    loss = torch.empty(E, device=dev)
+    work = torch.empty(workspace_floats(sizes.tolist(), args.history), device=dev)
+    nmax = int(sizes.max())
+    for _ in range(2):
+        relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    e0.record()
+    for _ in range(reps):
+        relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    relax_s = e0.elapsed_time(e1) / 1e3 / reps
+    # LUT cost kernel alone: algorithmic bytes = 8 corners x 4 B per near pair
+    cost = torch.empty(E, device=dev)
+    grad = torch.empty_like(flat)
+    pack_cuda_lut.overlap_multi_ensemble_ragged(flat, off, cost, lut, grad, n_max=nmax)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(10):
+        pack_cuda_lut.overlap_multi_ensemble_ragged(flat, off, cost, lut, grad, n_max=nmax)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    lut_ms = e0.elapsed_time(e1) / 10
+    near = 0
+    for k in range(0, E, max(1, E // 256)):      # sampled near-pair count
+        xk = xs[k]
+        dx = xk[:, None, :2] - xk[None, :, :2]
+        near += int(((dx ** 2).sum(-1) <= (2 * 0.5796198) ** 2).sum() - len(xk)) // 2
+    near_total = near * (E / len(range(0, E, max(1, E // 256))))
+    return {"instances": E, "n_range": [int(sizes.min()), int(sizes.max())], "lut_shape": list(lut.lut_d.shape),
+            "lut_build_s": build_s, "relaxations_per_s": E / relax_s, "ms_per_launch": relax_s * 1e3,
+            "launches": 1, "iterations": args.iters,
+            "lut_cost_kernel_ms": lut_ms,
+            "lut_kernel_algorithmic_GBps": near_total * 32 / (lut_ms * 1e-3) / 1e9,
+            "note": "one ragged launch (largest first); LUT tabulates the overlap area"}
+
+
+def measure_ga_step(args, dev):
+    """2048 packings of n = 100: Hungarian matching on 100 x 100 costs,
+    crossover + Gaussian mutation (0.05, 5 deg), 100-iteration relaxation."""
+    import torch
+
+    from packing_b200 import lap_batch
+    from packing_b200.ga_step import generation_step, matching_costs
+    P, n = args.ga_P, 100
+    xyt, h = workload(P, n, seed=21)
+    pop = torch.from_numpy(xyt).to(dev)
+    hh = torch.from_numpy(h).to(dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(0)
+    partners = torch.randperm(P, generator=gen, device=dev)
+    C = matching_costs(pop, pop[partners])
+    lap_batch.solve_lap_batch(C)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        lap_batch.solve_lap_batch(C)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    lap_ms = e0.elapsed_time(e1) / 3
+    generation_step(pop, partners, hh, gen, iterations=args.ga_iters)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    out, loss, rm = generation_step(pop, partners, hh, gen, iterations=args.ga_iters)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    step_ms = e0.elapsed_time(e1)
+    return {"population": P, "n": n, "lap_instances_per_s": P / (lap_ms * 1e-3), "lap_ms": lap_ms,
+            "lap_hbm_GBps": P * n * n * 4 / (lap_ms * 1e-3) / 1e9, "generation_ms": step_ms,
+            "generations_per_s": 1e3 / step_ms, "relax_iterations": args.ga_iters}
 
 
 def run_reference(args, rank, world):
@@ -333,10 +517,19 @@ def main():
     ap.add_argument("--history", type=int, default=10)
     ap.add_argument("--e2e-steps", dest="e2e_steps", type=int, default=2)
     ap.add_argument("--plain-E", dest="plain_E", type=int, default=4096)
-    ap.add_argument("--cpu-E", dest="cpu_E", type=int, default=8)
-    ap.add_argument("--ref-E", dest="ref_E", type=int, default=4)
+    ap.add_argument("--cpu-E", dest="cpu_E", type=int, default=128)
+    ap.add_argument("--ref-E", dest="ref_E", type=int, default=64)
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-extra", action="store_true", help="skip serving / ragged LUT / GA step")
+    ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=10000)
+    ap.add_argument("--serve-burst", dest="serve_burst", type=int, default=2000)
+    ap.add_argument("--serve-chunk", dest="serve_chunk", type=int, default=25)
+    ap.add_argument("--serve-plain", dest="serve_plain", type=int, default=512)
+    ap.add_argument("--serve-plain-batch", dest="serve_plain_batch", type=int, default=256)
+    ap.add_argument("--lut-E", dest="lut_E", type=int, default=8192)
+    ap.add_argument("--ga-P", dest="ga_P", type=int, default=2048)
+    ap.add_argument("--ga-iters", dest="ga_iters", type=int, default=100)
     ap.add_argument("--quick", action="store_true", help="headline timing only")
     args = ap.parse_args()
 
