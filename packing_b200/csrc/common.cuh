@@ -114,7 +114,7 @@ __device__ __forceinline__ T pk_block_max(T v, T* scratch)
     return r;
 }
 
-// Order-fixed vector reductions.  Element k belongs to group k / 256 and
+// Order-fixed vector reductions.  Element k belongs to group k / 64 and
 // lane k % 32; thread (warp w, lane l) OWNS the elements of the groups
 // g = w, w + nwarps, ... with lane l, and PK_OWN_LOOP visits exactly those.
 // Vector updates written with the same ownership need no barrier before the
@@ -123,7 +123,7 @@ __device__ __forceinline__ T pk_block_max(T v, T* scratch)
 // depends on N alone, not on blockDim.  red: two buffers of 32 * ngroups
 // entries, alternated by `flip` (one barrier per sum).  All threads call it
 // and all get the sum.
-#define PK_CANON_GROUP 256
+#define PK_CANON_GROUP 64
 #define PK_OWN_LOOP(k, N)                                                                      \
     for (int _g = (int)(threadIdx.x >> 5); _g * PK_CANON_GROUP < (N); _g += (int)(blockDim.x >> 5)) \
         for (int k = _g * PK_CANON_GROUP + (int)(threadIdx.x & 31);                             \

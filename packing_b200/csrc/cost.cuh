@@ -37,7 +37,7 @@ struct PkCostSmem {
 };
 
 // Pairs each thread tests per enumeration round.
-#define PK_PAIRS_PER_THREAD 8
+#define PK_PAIRS_PER_THREAD 4
 
 // List capacities: a round appends at most PK_PAIRS_PER_THREAD * T near
 // pairs, an expansion chunk at most 16 T piece pairs (T for the LUT, whose
