@@ -114,7 +114,65 @@ __device__ __forceinline__ T pk_block_max(T v, T* scratch)
     return r;
 }
 
-// Order-fixed vector reductions.  Element k belongs to group k / 64 and
+// Block-wide maximum of four floats at once (one round trip through
+// shared memory); scratch needs 4 * warps floats.  All threads get the result.
+__device__ __forceinline__ float4 pk_block_max4(float4 v, float* scratch)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x = fmaxf(v.x, __shfl_xor_sync(PK_FULL_MASK, v.x, o));
+        v.y = fmaxf(v.y, __shfl_xor_sync(PK_FULL_MASK, v.y, o));
+        v.z = fmaxf(v.z, __shfl_xor_sync(PK_FULL_MASK, v.z, o));
+        v.w = fmaxf(v.w, __shfl_xor_sync(PK_FULL_MASK, v.w, o));
+    }
+    __syncthreads();
+    if (lane == 0) {
+        scratch[4 * warp + 0] = v.x; scratch[4 * warp + 1] = v.y;
+        scratch[4 * warp + 2] = v.z; scratch[4 * warp + 3] = v.w;
+    }
+    __syncthreads();
+    float4 r = v;
+    for (int w = 0; w < nw; ++w) {
+        r.x = fmaxf(r.x, scratch[4 * w + 0]); r.y = fmaxf(r.y, scratch[4 * w + 1]);
+        r.z = fmaxf(r.z, scratch[4 * w + 2]); r.w = fmaxf(r.w, scratch[4 * w + 3]);
+    }
+    __syncthreads();
+    return r;
+}
+
+// Exclusive prefix sum of in[0..count) into out[0..count], out[count] = total.
+// scratch needs 32 ints.  Called by all threads; ends with a barrier.
+__device__ __forceinline__ void pk_block_exclusive_scan(const int* in, int* out, int count, int* scratch)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    int carry = 0;
+    for (int base = 0; base < count; base += blockDim.x) {
+        const int k = base + threadIdx.x;
+        const int v = k < count ? in[k] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(PK_FULL_MASK, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) scratch[warp] = incl;
+        __syncthreads();
+        int woff = 0, tot = 0;
+        for (int w = 0; w < nw; ++w) {
+            const int s = scratch[w];
+            woff += w < warp ? s : 0;
+            tot += s;
+        }
+        if (k < count) out[k] = carry + woff + incl - v;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[count] = carry;
+    __syncthreads();
+}
+
+// Order-fixed vector reductions.  Element k belongs to group k / 128 and
 // lane k % 32; thread (warp w, lane l) OWNS the elements of the groups
 // g = w, w + nwarps, ... with lane l, and PK_OWN_LOOP visits exactly those.
 // Vector updates written with the same ownership need no barrier before the
@@ -123,7 +181,7 @@ __device__ __forceinline__ T pk_block_max(T v, T* scratch)
 // depends on N alone, not on blockDim.  red: two buffers of 32 * ngroups
 // entries, alternated by `flip` (one barrier per sum).  All threads call it
 // and all get the sum.
-#define PK_CANON_GROUP 64
+#define PK_CANON_GROUP 128
 #define PK_OWN_LOOP(k, N)                                                                      \
     for (int _g = (int)(threadIdx.x >> 5); _g * PK_CANON_GROUP < (N); _g += (int)(blockDim.x >> 5)) \
         for (int k = _g * PK_CANON_GROUP + (int)(threadIdx.x & 31);                             \

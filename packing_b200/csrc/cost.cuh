@@ -27,25 +27,32 @@ struct PkCostSmem {
     uint32_t* items;    // [cap_items] piece pairs: i | j << 11 | pi << 22 | pj << 24
     uint32_t* near;     // [cap_near] centre-culled pairs: i | j << 11
     int* count;         // items in the list
-    int* count_near;    // near pairs in the list
     double* red;        // [32]
     long long* redl;    // [32]
     float2* piece;      // [16]
     int* piece_nv;      // [4]
-    unsigned int* cnt;  // [4] enumerated pairs, near pairs, piece pairs, evaluations
-    int cap_items, cap_near;
+    unsigned int* cnt;  // [4] candidate pairs tested, near pairs, piece pairs, evaluations
+    int* cell_start;    // [grid_cap + 1] first sorted slot of each grid cell
+    int* cell_fill;     // [grid_cap] trees per cell, then a scratch cursor
+    int* sorted;        // [n_max] tree indices ordered by cell
+    int* tcell;         // [n_max] cell of each tree
+    int* near_cnt;      // [n_max] near pairs of each sorted position
+    int* near_start;    // [n_max + 1] their offsets (exclusive scan)
+    int cap_items, cap_near, grid_cap;
 };
 
-// Pairs each thread tests per enumeration round.
-#define PK_PAIRS_PER_THREAD 4
+// Cells of the broad-phase grid (each at least the interaction distance
+// wide): two per tree, at least 64, at most 1024.
+__host__ __device__ inline int pk_grid_cap(int n_max) { return n_max < 32 ? 64 : (n_max > 512 ? 1024 : 2 * n_max); }
 
-// List capacities: a round appends at most PK_PAIRS_PER_THREAD * T near
-// pairs, an expansion chunk at most 16 T piece pairs (T for the LUT, whose
-// items are the near pairs themselves); each list is flushed before the next
-// round could overflow it.
+// List capacities.  The near list takes 8 T pairs, at least the n_max - 1
+// pairs of one tree for every n_max that pk_cost_threads gives T for; an
+// expansion chunk appends at most 16 T piece pairs to the item list, which is
+// flushed before the next chunk could overflow it (the LUT's items are the
+// near pairs themselves).
 __host__ __device__ inline void pk_caps(int T, int mode, int* cap_near, int* cap_items)
 {
-    *cap_near = 2 * PK_PAIRS_PER_THREAD * T;
+    *cap_near = 8 * T;
     *cap_items = mode == PK_PAIR_LUT ? 0 : 20 * T;
 }
 
@@ -59,8 +66,9 @@ __host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap_near, in
     b += (size_t)n_max * 4;         // theta
     b += (size_t)cap_items * 4;     // items
     b += (size_t)cap_near * 4;      // near pairs
-    b += 32 * 8 + 32 * 8 + 16 * 8 + 4 * 4 + 16 + 16 + 16;
-    return b;
+    b += (size_t)(2 * pk_grid_cap(n_max) + 1) * 4 + (size_t)n_max * 16 + 4;   // grid
+    b += 32 * 8 + 32 * 8 + 16 * 8 + 4 * 4 + 16 + 16 + 16 + 16;
+    return (b + 15) & ~(size_t)15;   // whatever follows starts 16-byte aligned
 }
 
 __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int cap_near, int cap_items)
@@ -70,17 +78,25 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
     s.pose = (float4*)p; p += (size_t)n_max * 16;
     s.bnd = (float4*)p; p += (size_t)n_max * 16;
     s.aabb = (float4*)p; p += (size_t)n_max * 64;
-    s.acc = (long long*)p; p += (size_t)n_max * 24;
+    // 8-byte arrays next: every offset up to here is a multiple of 16
     s.red = (double*)p; p += 32 * 8;
     s.redl = (long long*)p; p += 32 * 8;
+    s.acc = (long long*)p; p += (size_t)n_max * 24;
     s.piece = (float2*)p; p += 16 * 8;
     s.theta = (float*)p; p += (size_t)n_max * 4;
     s.items = (uint32_t*)p; p += (size_t)cap_items * 4;
     s.near = (uint32_t*)p; p += (size_t)cap_near * 4;
     s.piece_nv = (int*)p; p += 16;
     s.count = (int*)p; p += 16;
-    s.count_near = (int*)p; p += 16;
     s.cnt = (unsigned int*)p; p += 16;
+    s.grid_cap = pk_grid_cap(n_max);
+    s.cell_start = (int*)p; p += (size_t)(s.grid_cap + 1) * 4;
+    s.cell_fill = (int*)p; p += (size_t)s.grid_cap * 4;
+    s.sorted = (int*)p; p += (size_t)n_max * 4;
+    s.tcell = (int*)p; p += (size_t)n_max * 4;
+    s.near_cnt = (int*)p; p += (size_t)n_max * 4;
+    s.near_start = (int*)p; p += (size_t)n_max * 4 + 4;
+    p += 16;
     s.cap_items = cap_items;
     s.cap_near = cap_near;
     return s;
@@ -441,6 +457,97 @@ __device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, cons
     return tot;
 }
 
+// Centre-distance cull, rounded the same way wherever it is evaluated.
+__device__ __forceinline__ int pk_is_near(float4 A, float4 B, float cutoff)
+{
+    const float dx = __fsub_rn(B.x, A.x), dy = __fsub_rn(B.y, A.y);
+    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) <= cutoff;
+}
+
+// Sorted-position ranges [b0, b1) and [b2, b3) of the half neighbourhood of
+// sorted position a (grid of gx x gy cells, row-major cell order).
+__device__ __forceinline__ void pk_half_neighbourhood(const PkCostSmem& sm, int a, int gx, int gy, int& b0, int& b1,
+                                                      int& b2, int& b3)
+{
+    const int c = sm.tcell[sm.sorted[a]];
+    const int cy = c / gx, cx = c - cy * gx;
+    b0 = a + 1;
+    b1 = sm.cell_start[cy * gx + min(cx + 2, gx)];
+    if (cy + 1 < gy) {
+        const int r = (cy + 1) * gx;
+        b2 = sm.cell_start[r + max(cx - 1, 0)];
+        b3 = sm.cell_start[r + min(cx + 2, gx)];
+    } else {
+        b2 = b3 = b1;
+    }
+}
+
+// Processes the cn near pairs of the list: the LUT looks them up directly;
+// the analytic modes expand each into the piece pairs whose boxes overlap and
+// evaluate those in chunks.  All threads call it; it ends with a barrier.
+template <int MODE>
+__device__ __forceinline__ long long pk_flush_near(const PkCostSmem& sm, int cn, const PkCostSpec& spec, int T)
+{
+    long long tot = 0;
+    const int lane = threadIdx.x & 31;
+    if (MODE == PK_PAIR_LUT) {
+        if (threadIdx.x == 0) sm.cnt[2] += (unsigned)cn;
+        tot += pk_process_items<MODE>(sm, sm.near, cn, spec.w_pair, spec.lut);
+    } else {
+        for (int c0 = 0; c0 < cn; c0 += T) {
+            const int w = c0 + threadIdx.x;
+            uint32_t mask = 0, ij = 0;
+            if (w < cn) {
+                ij = sm.near[w];
+                const int i = ij & 2047, j = (ij >> 11) & 2047;
+                const float4 A = sm.pose[i], B = sm.pose[j];
+                const float dx = B.x - A.x, dy = B.y - A.y;
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const float4 a = sm.aabb[4 * i + p];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float4 b = sm.aabb[4 * j + q];
+                        const bool ov = !(a.y < b.x + dx || b.y + dx < a.x || a.w < b.z + dy || b.w + dy < a.z);
+                        mask |= (uint32_t)ov << (4 * p + q);
+                    }
+                }
+            }
+            const int cnt = __popc(mask);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(PK_FULL_MASK, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int wtot = __shfl_sync(PK_FULL_MASK, incl, 31);
+            int wbase = 0;
+            if (lane == 31 && wtot) {
+                wbase = atomicAdd(sm.count, wtot);
+                atomicAdd(&sm.cnt[2], (unsigned)wtot);
+            }
+            wbase = __shfl_sync(PK_FULL_MASK, wbase, 31);
+            int pos = wbase + incl - cnt;
+            while (mask) {
+                const int b = __ffs(mask) - 1;
+                mask &= mask - 1;
+                sm.items[pos++] = ij | ((uint32_t)(b >> 2) << 22) | ((uint32_t)(b & 3) << 24);
+            }
+            __syncthreads();
+            const int ci = *sm.count;
+            __syncthreads();
+            if (ci > sm.cap_items - 16 * T || c0 + T >= cn) {
+                tot += pk_process_items<MODE>(sm, sm.items, ci, spec.w_pair, spec.lut);
+                __syncthreads();
+                if (threadIdx.x == 0) *sm.count = 0;
+                __syncthreads();
+            }
+        }
+    }
+    __syncthreads();
+    return tot;
+}
+
 // Sum of v[0..n) in an order fixed by n alone (not by blockDim): lane l of
 // warp 0 adds its contiguous chunk, then a fixed shuffle tree.  Called by all
 // threads; returns the sum to all.
@@ -540,118 +647,107 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
     }
     if (threadIdx.x == 0) {
         *sm.count = 0;
-        *sm.count_near = 0;
         sm.cnt[3] += 1;
-        if (MODE != PK_PAIR_NONE && n > 1) sm.cnt[0] += (unsigned)(n * (n - 1) / 2);
     }
     __syncthreads();
 
     // ---- phases A + B: pairs -------------------------------------------------
     long long pair_tot = 0;
     if (MODE != PK_PAIR_NONE && n > 1) {
-        const int npairs = n * (n - 1) / 2;
         const float cutoff = c_geom.cutoff_sq;
-        const int lane = threadIdx.x & 31;
-        const unsigned lt = (1u << lane) - 1u;
-        const int span = PK_PAIRS_PER_THREAD * T;
-        // pair k = dd * n + i -> (i, (i + dd + 1) mod n); this thread's k
-        // advances by T, so (dd, i) advance by (T / n, T % n) with one carry
-        const int tdiv = T / n, tmod = T - (T / n) * n;
-        int cdd = threadIdx.x / n, ci = threadIdx.x - (threadIdx.x / n) * n;
-        for (int base = 0; base < npairs; base += span) {
-            // enumeration: PK_PAIRS_PER_THREAD pairs per thread, centre cull,
-            // survivors appended to the near list (one shared atomic per warp)
-#pragma unroll
-            for (int r = 0; r < PK_PAIRS_PER_THREAD; ++r) {
-                const int k = base + r * T + threadIdx.x;
-                bool nr = false;
-                uint32_t ij = 0;
-                const int i = ci;
-                int j = i + cdd + 1;
-                ci += tmod;
-                cdd += tdiv;
-                if (ci >= n) { ci -= n; ++cdd; }
-                if (k < npairs) {
-                    if (j >= n) j -= n;
-                    const float4 A = sm.pose[i], B = sm.pose[j];
-                    const float dx = B.x - A.x, dy = B.y - A.y;
-                    nr = dx * dx + dy * dy <= cutoff;
-                    ij = (uint32_t)i | ((uint32_t)j << 11);
-                }
-                const unsigned bal = __ballot_sync(PK_FULL_MASK, nr);
-                if (bal) {
-                    int wbase = 0;
-                    if (lane == 0) wbase = atomicAdd(sm.count_near, __popc(bal));
-                    wbase = __shfl_sync(PK_FULL_MASK, wbase, 0);
-                    if (nr) sm.near[wbase + __popc(bal & lt)] = ij;
+        // Broad phase on a uniform grid of cells at least the interaction
+        // distance wide: tree i only meets trees of the 3 x 3 cells around
+        // its own, and each pair is found once, from its lower index.
+        float4 bb = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, -3.4e38f);   // (-min x, max x, -min y, max y)
+        for (int t = threadIdx.x; t < n; t += T) {
+            const float4 A = sm.pose[t];
+            bb.x = fmaxf(bb.x, -A.x); bb.y = fmaxf(bb.y, A.x);
+            bb.z = fmaxf(bb.z, -A.y); bb.w = fmaxf(bb.w, A.y);
+        }
+        bb = pk_block_max4(bb, (float*)sm.red);
+        const float x0 = -bb.x, y0 = -bb.z;
+        const float wx = fmaxf(bb.y - x0, 0.f), wy = fmaxf(bb.w - y0, 0.f);
+        // 1 % wider than the interaction distance, so rounding in the cell
+        // index never puts two interacting trees two cells apart
+        float cs = sqrtf(cutoff) * 1.01f;
+        int gx = 1, gy = 1;
+        for (int tries = 0; tries < 64; ++tries) {
+            gx = (int)fminf(wx / cs, 2048.f) + 1;
+            gy = (int)fminf(wy / cs, 2048.f) + 1;
+            if (gx * gy <= sm.grid_cap) break;
+            cs *= 1.25f;
+        }
+        if (gx * gy > sm.grid_cap) { gx = 1; gy = 1; cs = 3.4e38f; }   // non-finite extent: one cell
+        const float inv = 1.0f / cs;
+        const int ncell = gx * gy;
+        for (int c = threadIdx.x; c < ncell; c += T) sm.cell_fill[c] = 0;
+        __syncthreads();
+        for (int t = threadIdx.x; t < n; t += T) {
+            const float4 A = sm.pose[t];
+            const int cx = min(gx - 1, max(0, (int)((A.x - x0) * inv)));
+            const int cy = min(gy - 1, max(0, (int)((A.y - y0) * inv)));
+            const int c = cy * gx + cx;
+            sm.tcell[t] = c;
+            atomicAdd(&sm.cell_fill[c], 1);
+        }
+        __syncthreads();
+        pk_block_exclusive_scan(sm.cell_fill, sm.cell_start, ncell, (int*)sm.redl);
+        for (int c = threadIdx.x; c < ncell; c += T) sm.cell_fill[c] = sm.cell_start[c];
+        __syncthreads();
+        for (int t = threadIdx.x; t < n; t += T) sm.sorted[atomicAdd(&sm.cell_fill[sm.tcell[t]], 1)] = t;
+        __syncthreads();
+
+        // Half neighbourhood of sorted position a in cell (cx, cy): the rest
+        // of its own cell and the cell to its right (one contiguous range of
+        // the sorted order), and cells cx-1..cx+1 of the row above (another).
+        // Every pair of trees in touching cells is found exactly once.
+        // Pass 1 counts the near pairs of each position, a scan turns the
+        // counts into list offsets, and pass 2 writes them in chunks that fit
+        // the near list, each chunk flushed before the next is written.
+        unsigned tested = 0;
+        for (int a = threadIdx.x; a < n; a += T) {
+            int b0, b1, b2, b3;
+            pk_half_neighbourhood(sm, a, gx, gy, b0, b1, b2, b3);
+            tested += (unsigned)(b1 - b0 + b3 - b2);
+            const float4 A = sm.pose[sm.sorted[a]];
+            int k = 0;
+            for (int b = b0; b < b1; ++b) k += pk_is_near(A, sm.pose[sm.sorted[b]], cutoff);
+            for (int b = b2; b < b3; ++b) k += pk_is_near(A, sm.pose[sm.sorted[b]], cutoff);
+            sm.near_cnt[a] = k;
+        }
+        __syncthreads();
+        pk_block_exclusive_scan(sm.near_cnt, sm.near_start, n, (int*)sm.redl);
+        atomicAdd(&sm.cnt[0], tested);
+        for (int a0 = 0; a0 < n;) {
+            // the longest run of positions from a0 whose pairs fit the list
+            // (a single position's pairs always do: cap_near >= n_max)
+            int lo = a0 + 1, hi = n;
+            const int lim = sm.near_start[a0] + sm.cap_near;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sm.near_start[mid] <= lim) lo = mid; else hi = mid - 1;
+            }
+            const int a1 = lo, base = sm.near_start[a0];
+            const int cn = sm.near_start[a1] - base;
+            for (int a = a0 + threadIdx.x; a < a1; a += T) {
+                int b0, b1, b2, b3;
+                pk_half_neighbourhood(sm, a, gx, gy, b0, b1, b2, b3);
+                const int ia = sm.sorted[a];
+                const float4 A = sm.pose[ia];
+                uint32_t* out = sm.near + (sm.near_start[a] - base);
+                const int kmax = sm.near_cnt[a];
+                int k = 0;
+                for (int b = b0; b < b3 && k < kmax; ++b) {
+                    if (b == b1) { b = b2; if (b >= b3) break; }
+                    const int ib = sm.sorted[b];
+                    if (pk_is_near(A, sm.pose[ib], cutoff))
+                        out[k++] = (uint32_t)min(ia, ib) | ((uint32_t)max(ia, ib) << 11);
                 }
             }
             __syncthreads();
-            const int cn = *sm.count_near;
-            __syncthreads();   // every thread has read the count before anyone appends again
-            if (cn > sm.cap_near - span || base + span >= npairs) {
-                if (threadIdx.x == 0) sm.cnt[1] += (unsigned)cn;
-                if (MODE == PK_PAIR_LUT) {
-                    // LUT items are the near pairs themselves
-                    if (threadIdx.x == 0) sm.cnt[2] += (unsigned)cn;
-                    pair_tot += pk_process_items<MODE>(sm, sm.near, cn, spec.w_pair, spec.lut);
-                } else {
-                    // expansion: 16 piece-pair AABB tests per near pair
-                    for (int c0 = 0; c0 < cn; c0 += T) {
-                        const int w = c0 + threadIdx.x;
-                        uint32_t mask = 0, ij = 0;
-                        if (w < cn) {
-                            ij = sm.near[w];
-                            const int i = ij & 2047, j = (ij >> 11) & 2047;
-                            const float4 A = sm.pose[i], B = sm.pose[j];
-                            const float dx = B.x - A.x, dy = B.y - A.y;
-#pragma unroll
-                            for (int p = 0; p < 4; ++p) {
-                                const float4 a = sm.aabb[4 * i + p];
-#pragma unroll
-                                for (int q = 0; q < 4; ++q) {
-                                    const float4 b = sm.aabb[4 * j + q];
-                                    const bool ov = !(a.y < b.x + dx || b.y + dx < a.x || a.w < b.z + dy ||
-                                                      b.w + dy < a.z);
-                                    mask |= (uint32_t)ov << (4 * p + q);
-                                }
-                            }
-                        }
-                        const int cnt = __popc(mask);
-                        int incl = cnt;
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const int v = __shfl_up_sync(PK_FULL_MASK, incl, o);
-                            if (lane >= o) incl += v;
-                        }
-                        const int wtot = __shfl_sync(PK_FULL_MASK, incl, 31);
-                        int wbase = 0;
-                        if (lane == 31 && wtot) {
-                            wbase = atomicAdd(sm.count, wtot);
-                            atomicAdd(&sm.cnt[2], (unsigned)wtot);
-                        }
-                        wbase = __shfl_sync(PK_FULL_MASK, wbase, 31);
-                        int pos = wbase + incl - cnt;
-                        while (mask) {
-                            const int b = __ffs(mask) - 1;
-                            mask &= mask - 1;
-                            sm.items[pos++] = ij | ((uint32_t)(b >> 2) << 22) | ((uint32_t)(b & 3) << 24);
-                        }
-                        __syncthreads();
-                        const int ci = *sm.count;
-                        __syncthreads();
-                        if (ci > sm.cap_items - 16 * T || c0 + T >= cn) {
-                            pair_tot += pk_process_items<MODE>(sm, sm.items, ci, spec.w_pair, spec.lut);
-                            __syncthreads();
-                            if (threadIdx.x == 0) *sm.count = 0;
-                            __syncthreads();
-                        }
-                    }
-                }
-                __syncthreads();
-                if (threadIdx.x == 0) *sm.count_near = 0;
-                __syncthreads();
-            }
+            if (threadIdx.x == 0) sm.cnt[1] += (unsigned)cn;
+            if (cn > 0) pair_tot += pk_flush_near<MODE>(sm, cn, spec, T);
+            a0 = a1;
         }
     }
 

@@ -176,6 +176,39 @@ def test_edge_cases(cuda):
         _overlap(poses(1, 1025, seed=9), False, cuda)
 
 
+@pytest.mark.parametrize("layout", ["cluster", "line", "spread", "cluster1024"])
+def test_broad_phase_layouts_vs_oracle(cuda, layout):
+    """Layouts that stress the cell grid: every pair near (the near list is
+    written in many chunks), a single row of cells, an extent far larger than
+    the grid (cells grow), and the maximum size fully clustered."""
+    rng = np.random.default_rng(11)
+    if layout == "cluster":
+        n = 300
+        x = np.concatenate([rng.uniform(-0.15, 0.15, (1, n, 2)), rng.uniform(0, 6.3, (1, n, 1))], axis=2)
+    elif layout == "line":
+        n = 400
+        x = np.stack([np.arange(n) * 0.3, rng.uniform(-0.05, 0.05, n), rng.uniform(0, 6.3, n)], axis=1)[None]
+    elif layout == "spread":
+        n = 256
+        x = np.concatenate([rng.uniform(-1000, 1000, (1, n, 2)), rng.uniform(0, 6.3, (1, n, 1))], axis=2)
+        x[0, 1::2, :2] = x[0, 0::2, :2] + rng.uniform(-0.4, 0.4, (n // 2, 2))   # overlapping pairs
+    else:
+        n = 1024
+        x = np.concatenate([rng.uniform(-0.5, 0.5, (1, n, 2)), rng.uniform(0, 6.3, (1, n, 1))], axis=2)
+    x = x.astype(np.float32)
+    # 1024 trees in a unit square: every tree overlaps ~1000 others, many of
+    # them nearly coincident, and float32 clipping of such pairs is
+    # ill-conditioned; a missed or doubled pair would still move a gradient
+    # by O(0.1), far above this bound
+    tol = 1e-2 if layout == "cluster1024" else TOL_GRAD
+    for use_sep in (False, True):
+        c, g = _overlap(x, use_sep, cuda)
+        oc, og = O.pair_cost(x.astype(np.float64), use_sep)
+        np.testing.assert_allclose(c, oc, rtol=RTOL_COST, atol=1e-6)
+        np.testing.assert_allclose(g, og, rtol=TOL_GRAD, atol=tol)
+        assert float(np.abs(g - og).mean()) < TOL_GRAD
+
+
 def test_argument_errors(cuda):
     from packing_b200 import pack_cuda
     x = torch.zeros((2, 4, 3), device=cuda)
