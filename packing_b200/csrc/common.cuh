@@ -172,43 +172,139 @@ __device__ __forceinline__ void pk_block_exclusive_scan(const int* in, int* out,
     __syncthreads();
 }
 
+// Elementwise arithmetic rounded after every operation (never contracted
+// into an FMA), as the reference's separate tensor operations round
+// (lbfgs_torch_parallel.py:546-690).
+__device__ __forceinline__ float pk_rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double pk_rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float pk_radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double pk_radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float pk_rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double pk_rsub(double a, double b) { return __dsub_rn(a, b); }
+
 // Order-fixed vector reductions.  Element k belongs to group k / 128 and
 // lane k % 32; thread (warp w, lane l) OWNS the elements of the groups
 // g = w, w + nwarps, ... with lane l, and PK_OWN_LOOP visits exactly those.
 // Vector updates written with the same ownership need no barrier before the
 // next reduction.  pk_canon_sum adds each group's per-lane partial in k
 // order, then the groups in order, then a fixed shuffle tree, so the sum
-// depends on N alone, not on blockDim.  red: two buffers of 32 * ngroups
-// entries, alternated by `flip` (one barrier per sum).  All threads call it
-// and all get the sum.
+// depends on N alone, not on blockDim.  red: two buffers of 64 * ngroups
+// entries, alternated by `flip` (one barrier per reduction: a thread can only
+// write a buffer again after the next reduction's barrier, by which time every
+// thread has finished reading it).  All threads call these and all get the
+// result.
 #define PK_CANON_GROUP 128
 #define PK_OWN_LOOP(k, N)                                                                      \
     for (int _g = (int)(threadIdx.x >> 5); _g * PK_CANON_GROUP < (N); _g += (int)(blockDim.x >> 5)) \
         for (int k = _g * PK_CANON_GROUP + (int)(threadIdx.x & 31);                             \
              k < min((N), (_g + 1) * PK_CANON_GROUP); k += 32)
 
+__host__ __device__ inline int pk_canon_groups(int N) { return (N + PK_CANON_GROUP - 1) / PK_CANON_GROUP; }
+
+template <typename T>
+__device__ __forceinline__ T* pk_canon_buf(int ng, T* red, int& flip)
+{
+    T* buf = red + (flip ? 64 * ng : 0);
+    flip ^= 1;
+    return buf;
+}
+
+// Second half of a canonical sum: barrier, the groups' per-lane partials in
+// group order, then the shuffle tree.  buf holds ng * 32 partials.
+template <typename T>
+__device__ __forceinline__ T pk_canon_finish(const T* buf, int ng)
+{
+    const int lane = threadIdx.x & 31;
+    __syncthreads();
+    T r = T(0);
+    for (int grp = 0; grp < ng; ++grp) r = pk_radd(r, buf[grp * 32 + lane]);
+    return pk_warp_sum(r);
+}
+
 template <typename T, typename Get>
 __device__ __forceinline__ T pk_canon_sum(int N, Get get, T* red, int& flip)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nw = blockDim.x >> 5;
-    const int ng = (N + PK_CANON_GROUP - 1) / PK_CANON_GROUP;
-    T* buf = red + (flip ? 32 * ng : 0);
-    flip ^= 1;
+    const int ng = pk_canon_groups(N);
+    T* buf = pk_canon_buf(ng, red, flip);
     for (int grp = warp; grp < ng; grp += nw) {
         T s = T(0);
         const int end = min(N, (grp + 1) * PK_CANON_GROUP);
-        for (int k = grp * PK_CANON_GROUP + lane; k < end; k += 32) s += get(k);
+        for (int k = grp * PK_CANON_GROUP + lane; k < end; k += 32) s = pk_radd(s, get(k));
         buf[grp * 32 + lane] = s;
     }
-    __syncthreads();
-    T r = T(0);
-    for (int grp = 0; grp < ng; ++grp) r += buf[grp * 32 + lane];
-    return pk_warp_sum(r);
+    return pk_canon_finish(buf, ng);
 }
 
-// Both buffers of pk_canon_sum (plus 32 entries of slack for block max).
-__host__ __device__ inline int pk_canon_red_len(int N) { return 2 * 32 * ((N + PK_CANON_GROUP - 1) / PK_CANON_GROUP) + 32; }
+// Two canonical sums with one barrier; each is bit-identical to its own
+// pk_canon_sum.
+template <typename T, typename Get>
+__device__ __forceinline__ void pk_canon_sum2(int N, Get get, T* red, int& flip, T& r0, T& r1)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    const int ng = pk_canon_groups(N);
+    T* buf = pk_canon_buf(ng, red, flip);
+    for (int grp = warp; grp < ng; grp += nw) {
+        T s0 = T(0), s1 = T(0);
+        const int end = min(N, (grp + 1) * PK_CANON_GROUP);
+        for (int k = grp * PK_CANON_GROUP + lane; k < end; k += 32) {
+            T a, b;
+            get(k, a, b);
+            s0 = pk_radd(s0, a);
+            s1 = pk_radd(s1, b);
+        }
+        buf[grp * 32 + lane] = s0;
+        buf[(ng + grp) * 32 + lane] = s1;
+    }
+    __syncthreads();
+    T a = T(0), b = T(0);
+    for (int grp = 0; grp < ng; ++grp) {
+        a = pk_radd(a, buf[grp * 32 + lane]);
+        b = pk_radd(b, buf[(ng + grp) * 32 + lane]);
+    }
+    r0 = pk_warp_sum(a);
+    r1 = pk_warp_sum(b);
+}
+
+// Maxima of two element functions over the owned elements with one barrier
+// (a maximum does not depend on the order).  Starts from 0: the callers
+// reduce absolute values.
+template <typename T, typename Get>
+__device__ __forceinline__ void pk_canon_max2(int N, Get get, T* red, int& flip, T& r0, T& r1)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    T* buf = pk_canon_buf(pk_canon_groups(N), red, flip);
+    T a = T(0), b = T(0);
+    PK_OWN_LOOP(k, N) {
+        T u, v;
+        get(k, u, v);
+        a = fmax(a, u);
+        b = fmax(b, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a = fmax(a, __shfl_xor_sync(PK_FULL_MASK, a, o));
+        b = fmax(b, __shfl_xor_sync(PK_FULL_MASK, b, o));
+    }
+    if (lane == 0) {
+        buf[2 * warp] = a;
+        buf[2 * warp + 1] = b;
+    }
+    __syncthreads();
+    for (int w = 0; w < nw; ++w) {
+        a = fmax(a, buf[2 * w]);
+        b = fmax(b, buf[2 * w + 1]);
+    }
+    r0 = a;
+    r1 = b;
+}
+
+// Both buffers of the canonical reductions (2 x 64 per group; a block of at
+// most 32 warps fits the per-warp maxima in one buffer).
+__host__ __device__ inline int pk_canon_red_len(int N) { return 2 * 64 * pk_canon_groups(N); }
 
 // Bounded wrap of an angle difference into [-pi, pi], following the
 // reference's subtract-2pi loop (pack_cuda_lut.py:289-293) in FP32.  Angles

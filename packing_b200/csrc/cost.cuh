@@ -157,19 +157,30 @@ __device__ __forceinline__ bool pk_clip_pass(const float2 (&X)[4], bool x_tri, c
 {
     const float tiny = c_geom.coll_tiny;
     const unsigned lines = y_tri ? 0x7u : 0xFu;
-    unsigned out[4], nearm[4];
+    unsigned out[4], nearm[4] = {0u, 0u, 0u, 0u};
+    float mn = 3.4e38f;   // smallest |f| against Y's real lines
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        unsigned o = 0, nm = 0;
+        unsigned o = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             o |= (unsigned)(f[k][v] < 0.f) << k;
-            nm |= (unsigned)(fabsf(f[k][v]) <= tiny) << k;
+            mn = fminf(mn, (k == 3 && y_tri) ? 3.4e38f : fabsf(f[k][v]));
         }
         out[v] = o & lines;
-        nearm[v] = nm & lines;
     }
     if (out[0] & out[1] & out[2] & out[3]) return false;
+    if (mn <= tiny) {
+        // some vertex lies within the tolerance of a line: the per-vertex
+        // masks of near lines (rarely needed, so built only here)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            unsigned nm = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) nm |= (unsigned)(fabsf(f[k][v]) <= tiny) << k;
+            nearm[v] = nm & lines;
+        }
+    }
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
         if (v == 3 && x_tri) break;
@@ -376,11 +387,26 @@ __device__ __forceinline__ float pk_lut_lookup(const PkLut& L, float x, float y,
     return val;
 }
 
+// Adds v to the int64 at a (shared memory) with two 32-bit atomics: the low
+// word's old value gives the carry, which travels with the high word.  The
+// sum stays exact modulo 2^64 whatever the interleaving (the carries total
+// floor((lo0 + sum lo_k) / 2^32) in any order), and a high-word add of zero
+// -- small values of either sign -- is skipped.  On this GPU a 64-bit
+// shared atomic costs several times two 32-bit ones.
+__device__ __forceinline__ void pk_fx_add(long long* a, long long v)
+{
+    unsigned* w = (unsigned*)a;   // little endian: w[0] low word, w[1] high word
+    const unsigned lo = (unsigned)v, hi = (unsigned)((unsigned long long)v >> 32);
+    const unsigned old = atomicAdd(&w[0], lo);
+    const unsigned up = hi + (unsigned)(old + lo < old);
+    if (up) atomicAdd(&w[1], up);
+}
+
 __device__ __forceinline__ void pk_acc_add(long long* acc, int t, float3 g)
 {
-    atomicAdd((unsigned long long*)&acc[3 * t + 0], (unsigned long long)pk_to_fx(g.x));
-    atomicAdd((unsigned long long*)&acc[3 * t + 1], (unsigned long long)pk_to_fx(g.y));
-    atomicAdd((unsigned long long*)&acc[3 * t + 2], (unsigned long long)pk_to_fx(g.z));
+    pk_fx_add(&acc[3 * t + 0], pk_to_fx(g.x));
+    pk_fx_add(&acc[3 * t + 1], pk_to_fx(g.y));
+    pk_fx_add(&acc[3 * t + 2], pk_to_fx(g.z));
 }
 
 __device__ __forceinline__ void pk_load_piece(const PkCostSmem& sm, int p, float c, float s, float ox,
@@ -548,23 +574,19 @@ __device__ __forceinline__ long long pk_flush_near(const PkCostSmem& sm, int cn,
     return tot;
 }
 
-// Sum of v[0..n) in an order fixed by n alone (not by blockDim): lane l of
-// warp 0 adds its contiguous chunk, then a fixed shuffle tree.  Called by all
-// threads; returns the sum to all.
-template <typename F>
-__device__ __forceinline__ double pk_canonical_sum(int n, F get, double* red)
+// Sums of the four components of bnd[0..n) in an order fixed by n alone
+// (not by blockDim): lane l of warp 0 adds its contiguous chunk in double,
+// then a fixed shuffle tree.  Called by warp 0 only; lane 0 gets the sums.
+__device__ __forceinline__ double4 pk_canonical_sum4(int n, const float4* bnd)
 {
-    double s = 0.0;
-    if (threadIdx.x < 32) {
-        const int k = (n + 31) >> 5;
-        const int b = threadIdx.x * k, e = min(n, b + k);
-        for (int t = b; t < e; ++t) s += get(t);
-        s = pk_warp_sum(s);
-        if (threadIdx.x == 0) red[0] = s;
+    double4 s = make_double4(0.0, 0.0, 0.0, 0.0);
+    const int k = (n + 31) >> 5;
+    const int b = threadIdx.x * k, e = min(n, b + k);
+    for (int t = b; t < e; ++t) {
+        const float4 v = bnd[t];
+        s.x += (double)v.x; s.y += (double)v.y; s.z += (double)v.z; s.w += (double)v.w;
     }
-    __syncthreads();
-    s = red[0];
-    __syncthreads();
+    s.x = pk_warp_sum(s.x); s.y = pk_warp_sum(s.y); s.z = pk_warp_sum(s.z); s.w = pk_warp_sum(s.w);
     return s;
 }
 
@@ -759,21 +781,27 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
             G[3 * t + 2] = (float)((double)sm.acc[3 * t + 2] * PK_FX_INV);
         }
     }
-    const long long ptot = pk_block_sum<long long>(pair_tot, sm.redl);
+    // one barrier for every total: per-warp pair partials (int64: exact in
+    // any order) and the boundary sums of warp 0
+    {
+        const long long wsum = pk_warp_sum(pair_tot);
+        if ((threadIdx.x & 31) == 0) sm.redl[threadIdx.x >> 5] = wsum;
+        if (do_bnd && threadIdx.x < 32) {
+            const double4 b4 = pk_canonical_sum4(n, sm.bnd);
+            if (threadIdx.x == 0) { sm.red[0] = b4.x; sm.red[1] = b4.y; sm.red[2] = b4.z; sm.red[3] = b4.w; }
+        }
+        __syncthreads();
+    }
+    long long ptot = 0;
+    for (int w = 0; w < (T >> 5); ++w) ptot += sm.redl[w];
     double total = (double)ptot * PK_FX_INV;
     double h0 = H ? (double)H[0] : 0.0;
     if (do_bnd) {
-        const double bsum = pk_canonical_sum(n, [&](int t) { return (double)sm.bnd[t].x; }, sm.red);
-        total += (double)spec.w_boundary * bsum;
-        if (GH) {
-            const double g0 = pk_canonical_sum(n, [&](int t) { return (double)sm.bnd[t].y; }, sm.red);
-            const double g1 = pk_canonical_sum(n, [&](int t) { return (double)sm.bnd[t].z; }, sm.red);
-            const double g2 = pk_canonical_sum(n, [&](int t) { return (double)sm.bnd[t].w; }, sm.red);
-            if (threadIdx.x == 0) {
-                GH[0] = (float)(spec.w_boundary * g0 + (double)spec.w_area * 2.0 * h0);
-                GH[1] = (float)(spec.w_boundary * g1);
-                GH[2] = (float)(spec.w_boundary * g2);
-            }
+        total += (double)spec.w_boundary * sm.red[0];
+        if (GH && threadIdx.x == 0) {
+            GH[0] = (float)(spec.w_boundary * sm.red[1] + (double)spec.w_area * 2.0 * h0);
+            GH[1] = (float)(spec.w_boundary * sm.red[2]);
+            GH[2] = (float)(spec.w_boundary * sm.red[3]);
         }
     } else if (GH && threadIdx.x == 0) {
         GH[0] = (float)((double)spec.w_area * 2.0 * h0);

@@ -17,44 +17,127 @@
 #include "common.cuh"
 #include "cost.cuh"
 
-template <typename F>
-__device__ __forceinline__ F pk_bmax(F v, F* red) { return pk_block_max<F>(v, red); }
-
 // Two-loop recursion (:533-572) for one system: d = -H g with the valid
 // history entries in logical order; al is shared scratch of m entries.
-// Vector work uses element ownership (PK_OWN_LOOP): no barrier besides the
-// one inside each reduction.
+// Every elementwise operation rounds as the reference's tensor operations do
+// (q - y a, s (al - be), products before the sums); the dot products use the
+// canonical order.  Vector work uses element ownership (PK_OWN_LOOP): no
+// barrier besides the one inside each reduction.
+//
+// When every warp owns at most one group (N <= 128 x warps), each thread
+// holds its <= 4 elements of q in registers and loads the next history entry
+// while the current dot product is being reduced, so the chain of 2 hlen
+// dependent reductions does not also wait for a memory round trip per step.
+// Both paths perform the same operations in the same order.
 template <typename F>
 __device__ void pk_two_loop(const F* g, F* d, int N, const F* S, const F* Y, const F* ro, int m, int hlen,
                             int hstart, F Hdiag, F* al, F* red, int& flip)
 {
-    PK_OWN_LOOP(k, N) d[k] = -g[k];
+    const int ng = pk_canon_groups(N);
+    const int nw = blockDim.x >> 5;
+    if (ng > nw) {
+        PK_OWN_LOOP(k, N) d[k] = -g[k];
+        for (int i = hlen - 1; i >= 0; --i) {
+            const int slot = (hstart + i) % m;
+            const F* s = S + (size_t)slot * N;
+            const F* y = Y + (size_t)slot * N;
+            const F a = pk_rmul(pk_canon_sum<F>(N, [&](int k) { return pk_rmul(s[k], d[k]); }, red, flip), ro[slot]);
+            if (threadIdx.x == 0) al[i] = a;
+            PK_OWN_LOOP(k, N) d[k] = pk_rsub(d[k], pk_rmul(y[k], a));
+        }
+        PK_OWN_LOOP(k, N) d[k] = pk_rmul(d[k], Hdiag);
+        __syncthreads();   // al[] visible
+        for (int i = 0; i < hlen; ++i) {
+            const int slot = (hstart + i) % m;
+            const F* s = S + (size_t)slot * N;
+            const F* y = Y + (size_t)slot * N;
+            const F be = pk_rmul(pk_canon_sum<F>(N, [&](int k) { return pk_rmul(y[k], d[k]); }, red, flip), ro[slot]);
+            const F c = pk_rsub(al[i], be);
+            PK_OWN_LOOP(k, N) d[k] = pk_radd(d[k], pk_rmul(s[k], c));
+        }
+        return;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int k0 = warp * PK_CANON_GROUP + lane;   // >= N for a warp that owns no group
+    F q[4], sc[4], yc[4], sn[4], yn[4];
+    F rc = 0, rn = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        q[j] = k0 + 32 * j < N ? -g[k0 + 32 * j] : F(0);
+        sc[j] = yc[j] = sn[j] = yn[j] = F(0);
+    }
+    auto fetch = [&](int i, F (&sv)[4], F (&yv)[4], F& r) {
+        const int slot = (hstart + i) % m;
+        const F* s = S + (size_t)slot * N;
+        const F* y = Y + (size_t)slot * N;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (k0 + 32 * j < N) {
+                sv[j] = s[k0 + 32 * j];
+                yv[j] = y[k0 + 32 * j];
+            }
+        }
+        r = ro[slot];
+    };
+    if (hlen > 0) fetch(hlen - 1, sc, yc, rc);
     for (int i = hlen - 1; i >= 0; --i) {
-        const int slot = (hstart + i) % m;
-        const F* s = S + (size_t)slot * N;
-        const F* y = Y + (size_t)slot * N;
-        const F a = pk_canon_sum<F>(N, [&](int k) { return s[k] * d[k]; }, red, flip) * ro[slot];
+        if (i > 0) fetch(i - 1, sn, yn, rn);
+        F* buf = pk_canon_buf(ng, red, flip);
+        if (warp < ng) {
+            F p = F(0);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (k0 + 32 * j < N) p = pk_radd(p, pk_rmul(sc[j], q[j]));
+            buf[warp * 32 + lane] = p;
+        }
+        const F a = pk_rmul(pk_canon_finish(buf, ng), rc);
         if (threadIdx.x == 0) al[i] = a;
-        PK_OWN_LOOP(k, N) d[k] = d[k] - y[k] * a;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            q[j] = pk_rsub(q[j], pk_rmul(yc[j], a));
+            sc[j] = sn[j];
+            yc[j] = yn[j];
+        }
+        rc = rn;
     }
-    PK_OWN_LOOP(k, N) d[k] = d[k] * Hdiag;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) q[j] = pk_rmul(q[j], Hdiag);
     __syncthreads();   // al[] visible
+    if (hlen > 0) fetch(0, sc, yc, rc);
     for (int i = 0; i < hlen; ++i) {
-        const int slot = (hstart + i) % m;
-        const F* s = S + (size_t)slot * N;
-        const F* y = Y + (size_t)slot * N;
-        const F be = pk_canon_sum<F>(N, [&](int k) { return y[k] * d[k]; }, red, flip) * ro[slot];
-        const F c = al[i] - be;
-        PK_OWN_LOOP(k, N) d[k] = d[k] + s[k] * c;
+        if (i + 1 < hlen) fetch(i + 1, sn, yn, rn);
+        F* buf = pk_canon_buf(ng, red, flip);
+        if (warp < ng) {
+            F p = F(0);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (k0 + 32 * j < N) p = pk_radd(p, pk_rmul(yc[j], q[j]));
+            buf[warp * 32 + lane] = p;
+        }
+        const F be = pk_rmul(pk_canon_finish(buf, ng), rc);
+        const F c = pk_rsub(al[i], be);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            q[j] = pk_radd(q[j], pk_rmul(sc[j], c));
+            sc[j] = sn[j];
+            yc[j] = yn[j];
+        }
+        rc = rn;
     }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (k0 + 32 * j < N) d[k0 + 32 * j] = q[j];
 }
 
+// max_k |v[k] * scale| and max_k |w[k] * wscale| with one barrier.
 template <typename F>
-__device__ __forceinline__ F pk_own_absmax(int N, const F* v, F scale, F* red)
+__device__ __forceinline__ void pk_own_absmax2(int N, const F* v, F scale, const F* w, F wscale, F* red, int& flip,
+                                               F& rv, F& rw)
 {
-    F p = 0;
-    PK_OWN_LOOP(k, N) p = fmax(p, (F)fabs(v[k] * scale));
-    return pk_bmax<F>(p, red + 2 * 32 * ((N + PK_CANON_GROUP - 1) / PK_CANON_GROUP));
+    pk_canon_max2<F>(N, [&](int k, F& a, F& b) {
+        a = (F)fabs(pk_rmul(v[k], scale));
+        b = (F)fabs(pk_rmul(w[k], wscale));
+    }, red, flip, rv, rw);
 }
 
 // ---------------------------------------------------------------------------
@@ -104,10 +187,11 @@ __global__ void pk_lbfgs_direction_kernel(PkLbfgsState<F> s, int n_iter, F lr, F
         t = lr;
     }
     if (has_max_step) {
-        const F pc = pk_own_absmax<F>(N, d, t, red);
+        F pc, unused;
+        pk_own_absmax2<F>(N, d, t, d, t, red, flip, pc, unused);
         if (pc > max_step) t = t * (max_step / pc);
     }
-    const F gtd = pk_canon_sum<F>(N, [&](int k) { return g[k] * d[k]; }, red, flip);
+    const F gtd = pk_canon_sum<F>(N, [&](int k) { return pk_rmul(g[k], d[k]); }, red, flip);
     if (gtd > -tol_change) active = 0;
     if (threadIdx.x == 0) {
         s.t[b] = t;
@@ -125,7 +209,7 @@ __global__ void pk_lbfgs_step_kernel(F* x, const F* d, const F* t, int M, int N)
 {
     const size_t total = (size_t)M * N;
     for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < total; w += (size_t)gridDim.x * blockDim.x)
-        x[w] = x[w] + t[w / N] * d[w];
+        x[w] = pk_radd(x[w], pk_rmul(t[w / N], d[w]));
 }
 
 // Phase 3 (:636-724): history update with the curvature guard, then the
@@ -147,8 +231,12 @@ __global__ void pk_lbfgs_update_kernel(PkLbfgsState<F> s, int n_iter, F tol_grad
     int active = s.active[b];
     int evals = s.evals[b] + 1;
     if (n_iter > 1) {
-        const F ys = pk_canon_sum<F>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red, flip);
-        const F yy = pk_canon_sum<F>(N, [&](int k) { const F y = g[k] - pg[k]; return y * y; }, red, flip);
+        F ys, yy;
+        pk_canon_sum2<F>(N, [&](int k, F& a, F& c) {
+            const F y = pk_rsub(g[k], pg[k]);
+            a = pk_rmul(y, pk_rmul(d[k], t));
+            c = pk_rmul(y, y);
+        }, red, flip, ys, yy);
         if (active && ys > (F)1e-10) {
             int hl = s.hlen[b], hs = s.hstart[b], slot;
             if (hl < m) { slot = (hs + hl) % m; ++hl; }
@@ -156,8 +244,8 @@ __global__ void pk_lbfgs_update_kernel(PkLbfgsState<F> s, int n_iter, F tol_grad
             F* S = s.S + ((size_t)b * m + slot) * N;
             F* Y = s.Y + ((size_t)b * m + slot) * N;
             PK_OWN_LOOP(k, N) {
-                Y[k] = g[k] - pg[k];
-                S[k] = d[k] * t;
+                Y[k] = pk_rsub(g[k], pg[k]);
+                S[k] = pk_rmul(d[k], t);
             }
             if (threadIdx.x == 0) {
                 s.H[b] = ys / yy;
@@ -167,8 +255,8 @@ __global__ void pk_lbfgs_update_kernel(PkLbfgsState<F> s, int n_iter, F tol_grad
             }
         }
     }
-    const F gmax = pk_own_absmax<F>(N, g, (F)1, red);
-    const F pc = pk_own_absmax<F>(N, d, t, red);
+    F gmax, pc;
+    pk_own_absmax2<F>(N, g, (F)1, d, t, red, flip, gmax, pc);
     if (threadIdx.x == 0) {
         if (gmax <= tol_grad) active = 0;
         if (evals >= max_eval) active = 0;
@@ -191,8 +279,11 @@ __global__ void pk_lbfgs_init_kernel(PkLbfgsState<F> s, F tol_grad)
 {
     extern __shared__ __align__(16) unsigned char pk_smem[];
     F* red = (F*)pk_smem;
+    int flip = 0;
     const int b = blockIdx.x;
-    const F gm = pk_own_absmax<F>(s.N, s.g + (size_t)b * s.N, (F)1, red);
+    const F* g = s.g + (size_t)b * s.N;
+    F gm, unused;
+    pk_own_absmax2<F>(s.N, g, (F)1, g, (F)1, red, flip, gm, unused);
     if (threadIdx.x == 0) {
         const int a = gm <= tol_grad ? 0 : 1;
         s.active[b] = a;
@@ -205,7 +296,13 @@ __global__ void pk_lbfgs_init_kernel(PkLbfgsState<F> s, F tol_grad)
     }
 }
 
-static inline int pk_lbfgs_threads(int N) { return N >= 1024 ? 256 : (N >= 256 ? 128 : 64); }
+// One warp per canonical group (so the two-loop keeps its elements in
+// registers), between 2 and 8 warps.
+static inline int pk_lbfgs_threads(int N)
+{
+    const int ng = pk_canon_groups(N);
+    return 32 * (ng < 2 ? 2 : (ng > 8 ? 8 : ng));
+}
 
 template <typename F>
 static int pk_lbfgs_phase(int phase, const PkLbfgsState<F>& s, int n_iter, double a, double b_, double c, double d_,
@@ -307,17 +404,20 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
             if (v.it == 0) {
                 // initial point (:489-500)
                 v.loss0 = v.loss;
-                const float gm = pk_own_absmax<float>(N, g, 1.f, red);
+                float gm, unused;
+                pk_own_absmax2<float>(N, g, 1.f, g, 1.f, red, flip, gm, unused);
                 v.active = !(gm <= prm.tol_grad);
             } else {
                 // after a step (:632-724)
                 ++v.evals;
                 if (v.it > 1) {
                     const float t = v.t;
-                    const float ys =
-                        pk_canon_sum<float>(N, [&](int k) { return (g[k] - pg[k]) * (d[k] * t); }, red, flip);
-                    const float yy = pk_canon_sum<float>(
-                        N, [&](int k) { const float y = g[k] - pg[k]; return y * y; }, red, flip);
+                    float ys, yy;
+                    pk_canon_sum2<float>(N, [&](int k, float& a, float& c) {
+                        const float y = pk_rsub(g[k], pg[k]);
+                        a = pk_rmul(y, pk_rmul(d[k], t));
+                        c = pk_rmul(y, y);
+                    }, red, flip, ys, yy);
                     if (ys > 1e-10f) {
                         int slot;
                         if (v.hlen < m) { slot = (v.hstart + v.hlen) % m; ++v.hlen; }
@@ -325,15 +425,15 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
                         float* Sd = S + (size_t)slot * N;
                         float* Yd = Y + (size_t)slot * N;
                         PK_OWN_LOOP(k, N) {
-                            Yd[k] = g[k] - pg[k];
-                            Sd[k] = d[k] * t;
+                            Yd[k] = pk_rsub(g[k], pg[k]);
+                            Sd[k] = pk_rmul(d[k], t);
                         }
                         v.H = ys / yy;
                         if (threadIdx.x == 0) ro[slot] = 1.f / ys;
                     }
                 }
-                const float gmax = pk_own_absmax<float>(N, g, 1.f, red);
-                const float pc = pk_own_absmax<float>(N, d, v.t, red);
+                float gmax, pc;
+                pk_own_absmax2<float>(N, g, 1.f, d, v.t, red, flip, gmax, pc);
                 if (gmax <= prm.tol_grad) v.active = 0;
                 if (v.evals >= prm.max_eval) v.active = 0;
                 if (pc <= prm.tol_change) v.active = 0;
@@ -367,13 +467,14 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
             t = prm.lr;
         }
         if (prm.has_max_step) {
-            const float pc = pk_own_absmax<float>(N, d, t, red);
+            float pc, unused;
+            pk_own_absmax2<float>(N, d, t, d, t, red, flip, pc, unused);
             if (pc > prm.max_step) t = t * (prm.max_step / pc);
         }
         v.t = t;
-        const float gtd = pk_canon_sum<float>(N, [&](int k) { return g[k] * d[k]; }, red, flip);
+        const float gtd = pk_canon_sum<float>(N, [&](int k) { return pk_rmul(g[k], d[k]); }, red, flip);
         if (gtd > -prm.tol_change) { v.active = 0; --v.it; return true; }
-        PK_OWN_LOOP(k, N) x[k] = x[k] + t * d[k];
+        PK_OWN_LOOP(k, N) x[k] = pk_radd(x[k], pk_rmul(t, d[k]));
         need_eval = v.it != prm.max_iter;
         if (!need_eval && prm.final_eval) {
             // the last step is not evaluated by the reference loop; evaluate once for the final loss
