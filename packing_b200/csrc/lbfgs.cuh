@@ -59,59 +59,75 @@ __device__ void pk_two_loop(const F* g, F* d, int N, const F* S, const F* Y, con
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int k0 = warp * PK_CANON_GROUP + lane;   // >= N for a warp that owns no group
+    // this lane's elements are k0 + 32 j for j < nv
+    const int nv = k0 < N ? min(4, (N - k0 + 31) >> 5) : 0;
+    const ptrdiff_t yoff = Y - S;                  // Y entry = S entry + yoff
     F q[4], sc[4], yc[4], sn[4], yn[4];
     F rc = 0, rn = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        q[j] = k0 + 32 * j < N ? -g[k0 + 32 * j] : F(0);
+        q[j] = j < nv ? -g[k0 + 32 * j] : F(0);
         sc[j] = yc[j] = sn[j] = yn[j] = F(0);
     }
-    auto fetch = [&](int i, F (&sv)[4], F (&yv)[4], F& r) {
-        const int slot = (hstart + i) % m;
-        const F* s = S + (size_t)slot * N;
-        const F* y = Y + (size_t)slot * N;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            if (k0 + 32 * j < N) {
-                sv[j] = s[k0 + 32 * j];
-                yv[j] = y[k0 + 32 * j];
-            }
-        }
-        r = ro[slot];
-    };
-    if (hlen > 0) fetch(hlen - 1, sc, yc, rc);
+#define PK_TL_FETCH(SV, YV, P)                         \
+    {                                                  \
+        _Pragma("unroll") for (int j = 0; j < 4; ++j)  \
+            if (j < nv) {                              \
+                SV[j] = (P)[32 * j];                   \
+                YV[j] = (P)[yoff + 32 * j];            \
+            }                                          \
+    }
+    // first loop: newest entry first; the slot steps down with wraparound
+    int slot = hlen > 0 ? (hstart + hlen - 1) % m : 0;
+    const F* pcur = S + (size_t)slot * N + k0;
+    if (hlen > 0) {
+        PK_TL_FETCH(sc, yc, pcur)
+        rc = ro[slot];
+    }
     for (int i = hlen - 1; i >= 0; --i) {
-        if (i > 0) fetch(i - 1, sn, yn, rn);
+        const int nslot = slot == 0 ? m - 1 : slot - 1;
+        const F* pnext = slot == 0 ? pcur + (size_t)(m - 1) * N : pcur - N;
+        if (i > 0) {
+            PK_TL_FETCH(sn, yn, pnext)
+            rn = ro[nslot];
+        }
         F* buf = pk_canon_buf(ng, red, flip);
         if (warp < ng) {
             F p = F(0);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (k0 + 32 * j < N) p = pk_radd(p, pk_rmul(sc[j], q[j]));
+                if (j < nv) p = pk_radd(p, pk_rmul(sc[j], q[j]));
             buf[warp * 32 + lane] = p;
         }
         const F a = pk_rmul(pk_canon_finish(buf, ng), rc);
         if (threadIdx.x == 0) al[i] = a;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            q[j] = pk_rsub(q[j], pk_rmul(yc[j], a));
-            sc[j] = sn[j];
-            yc[j] = yn[j];
+        for (int j = 0; j < 4; ++j) q[j] = pk_rsub(q[j], pk_rmul(yc[j], a));
+        if (i > 0) {   // entry 0 stays in hand: the second loop starts with it
+#pragma unroll
+            for (int j = 0; j < 4; ++j) { sc[j] = sn[j]; yc[j] = yn[j]; }
+            rc = rn;
+            slot = nslot;
+            pcur = pnext;
         }
-        rc = rn;
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) q[j] = pk_rmul(q[j], Hdiag);
     __syncthreads();   // al[] visible
-    if (hlen > 0) fetch(0, sc, yc, rc);
+    // second loop: oldest entry first; the slot steps up with wraparound
     for (int i = 0; i < hlen; ++i) {
-        if (i + 1 < hlen) fetch(i + 1, sn, yn, rn);
+        const int nslot = slot == m - 1 ? 0 : slot + 1;
+        const F* pnext = slot == m - 1 ? pcur - (size_t)(m - 1) * N : pcur + N;
+        if (i + 1 < hlen) {
+            PK_TL_FETCH(sn, yn, pnext)
+            rn = ro[nslot];
+        }
         F* buf = pk_canon_buf(ng, red, flip);
         if (warp < ng) {
             F p = F(0);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (k0 + 32 * j < N) p = pk_radd(p, pk_rmul(yc[j], q[j]));
+                if (j < nv) p = pk_radd(p, pk_rmul(yc[j], q[j]));
             buf[warp * 32 + lane] = p;
         }
         const F be = pk_rmul(pk_canon_finish(buf, ng), rc);
@@ -123,10 +139,13 @@ __device__ void pk_two_loop(const F* g, F* d, int N, const F* S, const F* Y, con
             yc[j] = yn[j];
         }
         rc = rn;
+        slot = nslot;
+        pcur = pnext;
     }
+#undef PK_TL_FETCH
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-        if (k0 + 32 * j < N) d[k0 + 32 * j] = q[j];
+        if (j < nv) d[k0 + 32 * j] = q[j];
 }
 
 // max_k |v[k] * scale| and max_k |w[k] * wscale| with one barrier.
