@@ -200,6 +200,11 @@ typedef struct PkRelaxParams {
     unsigned long long* counters;  /* device (6,) or NULL: enumerated pairs, near pairs,
                                       piece pairs, cost evaluations, iterations,
                                       history entries streamed -- accumulated */
+    int threads;              /* threads per packing: 0 = library default for n_max, else
+                                 a multiple of 32 in [32, 256] with 8 * threads >= n_max - 1
+                                 (an autotuned choice); results do not depend on it */
+    int persistent;           /* 1: one CTA per resident slot, each walking the launch
+                                 order with the grid's stride; 0: one CTA per packing */
 } PkRelaxParams;
 
 /* Fused batched relaxation (OptimizerBFGS.run_simulation,

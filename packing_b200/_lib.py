@@ -66,6 +66,7 @@ class PkRelaxParams(ctypes.Structure):
         ("tol_change", ctypes.c_float), ("tol_rel_change", ctypes.c_float),
         ("stop_on_cost_increase", ctypes.c_int), ("max_eval", ctypes.c_int), ("final_eval", ctypes.c_int),
         ("counters", ctypes.c_void_p),
+        ("threads", ctypes.c_int), ("persistent", ctypes.c_int),
     ]
 
 

@@ -17,6 +17,8 @@
 #include "common.cuh"
 #include "cost.cuh"
 
+#include <mutex>
+
 // Two-loop recursion (:533-572) for one system: d = -H g with the valid
 // history entries in logical order; al is shared scratch of m entries.
 // Every elementwise operation rounds as the reference's tensor operations do
@@ -504,15 +506,14 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
     }
 }
 
+// Relaxes instance e (all threads of the block call it; e is uniform).
 template <int MODE>
-__global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in,
-                                const int* __restrict__ offsets, const int* __restrict__ order, int E, int n_max,
-                                PkCostSpec spec, PkRelaxParams prm, float* __restrict__ xyt_out,
-                                float* __restrict__ h_out, float* __restrict__ loss_out, int* __restrict__ iters_out,
-                                float* __restrict__ work, int cap_near, int cap_items)
+__device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const float* __restrict__ h_in,
+                                  const int* __restrict__ offsets, int E, int n_max, const PkCostSpec& spec,
+                                  const PkRelaxParams& prm, float* __restrict__ xyt_out, float* __restrict__ h_out,
+                                  float* __restrict__ loss_out, int* __restrict__ iters_out, float* __restrict__ work,
+                                  int cap_near, int cap_items, unsigned char* smem)
 {
-    extern __shared__ __align__(16) unsigned char pk_smem[];
-    const int e = order ? order[blockIdx.x] : blockIdx.x;
     if (e < 0 || e >= E) return;
     const int base = offsets ? offsets[e] : e * n_max;
     const int n = offsets ? offsets[e + 1] - base : n_max;
@@ -523,9 +524,9 @@ __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restric
     const int N = 3 * n + 3;
     const int NM = 3 * n_max + 3;
     const int m = prm.history;
-    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap_near, cap_items);
+    PkCostSmem sm = pk_cost_carve(smem, n_max, cap_near, cap_items);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
-    float* x = (float*)(pk_smem + pk_cost_smem_bytes(n_max, cap_near, cap_items));
+    float* x = (float*)(smem + pk_cost_smem_bytes(n_max, cap_near, cap_items));
     float* g = x + NM;
     float* pg = g + NM;
     float* d = pg + NM;
@@ -556,6 +557,29 @@ __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restric
             atomicAdd(&prm.counters[4], (unsigned long long)v.it);
             atomicAdd(&prm.counters[5], hist_streamed * (unsigned long long)N);
         }
+    }
+}
+
+// One CTA per instance, or (persistent) one CTA per resident slot walking the
+// launch order with a stride of the grid: CTA b relaxes order[b],
+// order[b + G], ...; largest-first orders keep the CTAs' loads even.
+template <int MODE, bool PERSISTENT>
+__global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in,
+                                const int* __restrict__ offsets, const int* __restrict__ order, int E, int n_max,
+                                PkCostSpec spec, PkRelaxParams prm, float* __restrict__ xyt_out,
+                                float* __restrict__ h_out, float* __restrict__ loss_out, int* __restrict__ iters_out,
+                                float* __restrict__ work, int cap_near, int cap_items)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    if (!PERSISTENT) {
+        pk_relax_instance<MODE>(order ? order[blockIdx.x] : blockIdx.x, xyt_in, h_in, offsets, E, n_max, spec, prm,
+                                xyt_out, h_out, loss_out, iters_out, work, cap_near, cap_items, pk_smem);
+        return;
+    }
+    for (int k = blockIdx.x; k < E; k += gridDim.x) {
+        pk_relax_instance<MODE>(order ? order[k] : k, xyt_in, h_in, offsets, E, n_max, spec, prm, xyt_out, h_out,
+                                loss_out, iters_out, work, cap_near, cap_items, pk_smem);
+        __syncthreads();   // shared state is reused by the next instance
     }
 }
 
@@ -631,6 +655,82 @@ static size_t pk_relax_smem_bytes(int n_max, int cap_near, int cap_items, int m)
     return pk_cost_smem_bytes(n_max, cap_near, cap_items) + ((size_t)4 * NM + 2 * (size_t)m + pk_canon_red_len(NM)) * 4;
 }
 
+// Threads per CTA of the relaxation kernels: the caller's choice (an
+// autotuned value) or the default for the instance size.  Any multiple of 32
+// up to 256 gives the same results (every reduction has an order fixed by
+// the instance alone); the near list (8 T pairs) must hold one tree's n_max - 1.
+static int pk_relax_threads(int n_max, int want, int* T, const char* who)
+{
+    if (want == 0) {
+        *T = pk_cost_threads(n_max);
+        return PK_OK;
+    }
+    if (want < 32 || want > 256 || (want & 31)) {
+        snprintf(g_pk_err, sizeof(g_pk_err), "%s: threads must be 0 or a multiple of 32 in [32, 256], got %d", who,
+                 want);
+        return PK_EINVAL;
+    }
+    if (8 * want < n_max - 1) {
+        snprintf(g_pk_err, sizeof(g_pk_err), "%s: %d threads are too few for %d trees (need 8 * threads >= n - 1)",
+                 who, want, n_max);
+        return PK_EINVAL;
+    }
+    *T = want;
+    return PK_OK;
+}
+
+// Raises a kernel's dynamic shared memory limit only when a launch needs more
+// than any earlier one on this device, so warmed-up launches make no
+// attribute call (they can then be captured into a CUDA graph).
+static cudaError_t pk_set_smem(const void* fn, int slot, size_t smem)
+{
+    static size_t done[64][16];
+    static std::mutex mu;
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= 64 || slot < 0 || slot >= 16) return cudaErrorInvalidValue;
+    std::lock_guard<std::mutex> lock(mu);
+    if (smem <= done[dev][slot]) return cudaSuccess;
+    err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err == cudaSuccess) done[dev][slot] = smem;
+    return err;
+}
+
+// Grid of a persistent launch: every CTA the GPU can keep resident, at most
+// E.  The occupancy of a (kernel, threads, shared memory) shape is queried
+// once per device and remembered, so warmed-up launches make no query.
+static cudaError_t pk_resident_grid(const void* fn, int threads, size_t smem, int E, int* grid)
+{
+    struct Entry { const void* fn; int threads; size_t smem; int resident; };
+    static Entry cache[64][32];
+    static int used[64];
+    static std::mutex mu;
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidValue;
+    int resident = -1;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (int k = 0; k < used[dev]; ++k) {
+            const Entry& c = cache[dev][k];
+            if (c.fn == fn && c.threads == threads && c.smem == smem) { resident = c.resident; break; }
+        }
+    }
+    if (resident < 0) {
+        int sms = 0, per_sm = 0;
+        err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+        if (err != cudaSuccess) return err;
+        resident = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+        std::lock_guard<std::mutex> lock(mu);
+        if (used[dev] < 32) cache[dev][used[dev]++] = Entry{fn, threads, smem, resident};
+    }
+    *grid = resident < E ? resident : E;
+    return cudaSuccess;
+}
+
 extern "C" size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, int history)
 {
     size_t tot = 0;
@@ -657,19 +757,32 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
     if ((spec->w_boundary != 0.f || spec->w_area != 0.f) && !h_in)
         return pk_fail(PK_EINVAL, "pk_relax: boundary / area terms need h%s");
     if (spec->pair_mode == PK_PAIR_LUT && !spec->lut.vals) return pk_fail(PK_EINVAL, "pk_relax: LUT without vals%s");
-    const int T = pk_cost_threads(n_max);
+    int T = 0;
+    rc = pk_relax_threads(n_max, prm->threads, &T, "pk_relax");
+    if (rc) return rc;
     int cap_near, cap_items;
     pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
     const size_t smem = pk_relax_smem_bytes(n_max, cap_near, cap_items, prm->history);
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaSuccess;
+    int grid = E;
     switch (spec->pair_mode) {
 #define PK_R(M)                                                                                          \
     case M:                                                                                              \
-        err = cudaFuncSetAttribute(pk_relax_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        if (err == cudaSuccess)                                                                          \
-            pk_relax_kernel<M><<<E, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, xyt_out, \
-                                                   h_out, loss_out, iters_out, work, cap_near, cap_items); \
+        if (prm->persistent) {                                                                           \
+            err = pk_set_smem((const void*)pk_relax_kernel<M, true>, 12 + M, smem);                      \
+            if (err == cudaSuccess) err = pk_resident_grid((const void*)pk_relax_kernel<M, true>, T, smem, E, &grid); \
+            if (err == cudaSuccess)                                                                      \
+                pk_relax_kernel<M, true><<<grid, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, \
+                                                                xyt_out, h_out, loss_out, iters_out, work, cap_near, \
+                                                                cap_items);                              \
+        } else {                                                                                         \
+            err = pk_set_smem((const void*)pk_relax_kernel<M, false>, 4 + M, smem);                      \
+            if (err == cudaSuccess)                                                                      \
+                pk_relax_kernel<M, false><<<grid, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, \
+                                                                 xyt_out, h_out, loss_out, iters_out, work, cap_near, \
+                                                                 cap_items);                             \
+        }                                                                                                \
         break;
         PK_R(PK_PAIR_NONE)
         PK_R(PK_PAIR_AREA)
@@ -694,7 +807,9 @@ extern "C" int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* poo
     if (prm->history < 1 || prm->history > 64) return pk_fail(PK_EINVAL, "pk_relax_jobs: history must be in [1, 64]%s");
     if (!jobs || !list || !pool) return pk_fail(PK_EINVAL, "pk_relax_jobs: NULL pointer%s");
     if (spec->pair_mode == PK_PAIR_LUT && !spec->lut.vals) return pk_fail(PK_EINVAL, "pk_relax_jobs: LUT without vals%s");
-    const int T = pk_cost_threads(n_max);
+    int T = 0;
+    rc = pk_relax_threads(n_max, prm->threads, &T, "pk_relax_jobs");
+    if (rc) return rc;
     int cap_near, cap_items;
     pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
     const size_t smem = pk_relax_smem_bytes(n_max, cap_near, cap_items, prm->history);
@@ -703,7 +818,7 @@ extern "C" int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* poo
     switch (spec->pair_mode) {
 #define PK_J(M)                                                                                          \
     case M:                                                                                              \
-        err = cudaFuncSetAttribute(pk_relax_jobs_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        err = pk_set_smem((const void*)pk_relax_jobs_kernel<M>, 8 + M, smem);                            \
         if (err == cudaSuccess)                                                                          \
             pk_relax_jobs_kernel<M><<<njobs, T, smem, st>>>(jobs, list, njobs, pool, n_max, *spec, *prm, chunk_iters, \
                                                             cap_near, cap_items);                        \

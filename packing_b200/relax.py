@@ -38,6 +38,8 @@ class RelaxParams:
     max_eval: int | None = None
     final_eval: bool = True
     counters: object = None      # optional CUDA int64 tensor (6,), accumulated work counts
+    threads: int = 0             # threads per packing (0: library default; see tune.py)
+    persistent: bool = False     # one CTA per resident slot instead of one per packing
 
     def to_c(self) -> PkRelaxParams:
         p = PkRelaxParams()
@@ -53,6 +55,8 @@ class RelaxParams:
         p.max_eval = int(self.max_eval if self.max_eval is not None else self.n_iterations * 5 // 4)
         p.final_eval = int(bool(self.final_eval))
         p.counters = self.counters.data_ptr() if self.counters is not None else None
+        p.threads = int(self.threads)
+        p.persistent = int(bool(self.persistent))
         return p
 
 

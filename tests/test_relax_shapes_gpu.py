@@ -1,0 +1,110 @@
+"""Launch shapes of the fused relaxation: threads per packing and the
+persistent grid change the speed, never the result; the launch can be
+captured into a CUDA graph and replayed on new inputs; the autotuner picks
+a feasible shape and caches it."""
+import numpy as np
+import pytest
+import torch
+
+from tests.workloads import poses, square_h
+
+pytestmark = pytest.mark.gpu
+
+
+def _spec():
+    from packing_b200.cost import CostSpec
+    return CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
+
+
+def _run(xyt, h, prm, offsets=None, order=None, n_max=None):
+    from packing_b200.relax import relax_into, workspace_floats
+    sizes = [xyt.shape[1]] * xyt.shape[0] if offsets is None else list(np.diff(offsets.cpu().numpy()))
+    E = len(sizes)
+    xo, ho = torch.empty_like(xyt), torch.empty_like(h)
+    loss = torch.empty(E, device=xyt.device)
+    it = torch.empty(E, dtype=torch.int32, device=xyt.device)
+    work = torch.empty(workspace_floats(sizes, prm.history_size), device=xyt.device)
+    relax_into(xyt, h, xo, ho, loss, work, _spec(), prm, offsets=offsets, order=order, n_max=n_max, iters_out=it)
+    torch.cuda.synchronize()
+    return xo.cpu().numpy(), loss.cpu().numpy(), it.cpu().numpy()
+
+
+def test_threads_and_persistent_do_not_change_results(cuda):
+    from packing_b200.relax import RelaxParams
+    from packing_b200.tune import feasible_threads
+    E, n = 37, 60
+    xyt = torch.from_numpy(poses(E, n, seed=3)).to(cuda)
+    h = torch.from_numpy(square_h(E, n)).to(cuda)
+    ref = _run(xyt, h, RelaxParams(n_iterations=40, history_size=6, max_step=0.01))
+    for t in [32] + feasible_threads(n):
+        for p in (False, True):
+            out = _run(xyt, h, RelaxParams(n_iterations=40, history_size=6, max_step=0.01, threads=t, persistent=p))
+            for a, b in zip(ref, out):
+                assert np.array_equal(a, b), (t, p)
+
+
+def test_ragged_persistent_matches_one_cta_per_packing(cuda):
+    from packing_b200.relax import RelaxParams
+    rng = np.random.default_rng(5)
+    sizes = [int(s) for s in rng.integers(5, 90, size=300)]
+    flat = np.concatenate([poses(1, s, seed=100 + k)[0] for k, s in enumerate(sizes)]).astype(np.float32)
+    off = np.zeros(len(sizes) + 1, np.int32)
+    off[1:] = np.cumsum(sizes)
+    h = np.concatenate([square_h(1, s) for s in sizes]).astype(np.float32)
+    xt = torch.from_numpy(flat).to(cuda)
+    ht = torch.from_numpy(h).to(cuda)
+    offt = torch.from_numpy(off).to(cuda)
+    order = torch.tensor(sorted(range(len(sizes)), key=lambda e: -sizes[e]), dtype=torch.int32, device=cuda)
+    a = _run(xt, ht, RelaxParams(n_iterations=30, history_size=4), offsets=offt, order=order, n_max=max(sizes))
+    b = _run(xt, ht, RelaxParams(n_iterations=30, history_size=4, persistent=True, threads=96), offsets=offt,
+             order=order, n_max=max(sizes))
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_graph_capture_and_replay(cuda):
+    """The persistent launch captured once and replayed on new poses equals
+    eager launches on the same poses."""
+    from packing_b200.relax import RelaxParams, relax_into, workspace_floats
+    E, n = 64, 50
+    prm = RelaxParams(n_iterations=25, history_size=5, max_step=0.01, persistent=True)
+    x_static = torch.from_numpy(poses(E, n, seed=21)).to(cuda)
+    h_static = torch.from_numpy(square_h(E, n)).to(cuda)
+    xo, ho = torch.empty_like(x_static), torch.empty_like(h_static)
+    loss = torch.empty(E, device=cuda)
+    it = torch.empty(E, dtype=torch.int32, device=cuda)
+    work = torch.empty(workspace_floats([n] * E, prm.history_size), device=cuda)
+    side = torch.cuda.Stream(cuda)
+    side.wait_stream(torch.cuda.current_stream(cuda))
+    with torch.cuda.stream(side):   # warm-up off the capture: attributes and occupancy are set here
+        relax_into(x_static, h_static, xo, ho, loss, work, _spec(), prm, iters_out=it)
+    torch.cuda.current_stream(cuda).wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        relax_into(x_static, h_static, xo, ho, loss, work, _spec(), prm, iters_out=it)
+    for seed in (22, 23):
+        new = torch.from_numpy(poses(E, n, seed=seed)).to(cuda)
+        x_static.copy_(new)
+        g.replay()
+        torch.cuda.synchronize()
+        got = (xo.cpu().numpy(), loss.cpu().numpy(), it.cpu().numpy())
+        ref = _run(new, h_static, RelaxParams(n_iterations=25, history_size=5, max_step=0.01))
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b)
+    del g
+
+
+def test_tuner_picks_feasible_shape_and_caches(cuda, tmp_path):
+    from packing_b200.tune import RelaxTuner, feasible_threads
+    tn = RelaxTuner(cuda, cache_path=str(tmp_path / "tune.json"), iterations=3, reps=1)
+    t, p = tn.best(40, _spec(), 5)
+    assert t in feasible_threads(48) and isinstance(p, bool)
+    tn2 = RelaxTuner(cuda, cache_path=str(tmp_path / "tune.json"))
+
+    def boom(*a, **k):
+        raise AssertionError("cached shape was re-measured")
+    tn2.measure = boom
+    assert tn2.best(45, _spec(), 5) == (t, p)   # same bucket, read from the cache file
+    prm = tn2.tuned(__import__("packing_b200.relax", fromlist=["RelaxParams"]).RelaxParams(history_size=5), 45,
+                    _spec())
+    assert prm.threads == t and prm.persistent == p
