@@ -185,6 +185,34 @@ int pk_validate_fp64(const void* xyt, int dtype_bytes, int E, int n, int* overla
 int pk_lbfgs_phase(int phase, int dtype_bytes, void* const* arrays, int M, int N, int m, int n_iter, double p0,
                    double p1, double p2, double p3, int i1, int i2, void* stream);
 
+/* Batched strong-Wolfe line search of the drop-in lbfgs
+ * (_strong_wolfe_batched, lbfgs_torch_parallel.py:70-407, with its defaults
+ * c1 = 1e-4, c2 = 0.9, tolerance_change = 1e-9, max_ls = 25 as the main loop
+ * calls it, :613-617).  A per-system state machine run in phases by the
+ * host, which calls the objective between them on the rows the reference
+ * evaluates:
+ *   0 init (g . d, |d|max, first trial x + t d)      -> objective on rows with in_ls, is_main
+ *   1 after an evaluation (g_new . d, count; flag_arg = 1 for the first one)
+ *   2 bracketing pass (ls_iter)                       -> flag: any active -> objective on active rows
+ *   3 zoom start (flag_arg = 1 when the bracketing ran out of evaluations)
+ *   4 zoom pass before its evaluation (tol_change)   -> flag: any active -> objective on active rows
+ *   5 zoom bracket update after the evaluation
+ *   6 result: t, f_new, g_new of each searched system
+ * arrays: x, d, g, f, gtd, t, x_new, g_new, f_new, gtd_new, g_prev, f_prev,
+ * gtd_prev, t_prev, bg (M,2,N), bt, bf, bgtd (M,2), d_norm, t_new (dtype of
+ * dtype_bytes), then int32: bsize, done, active, low, insuf, evals, in_ls,
+ * flag (1).  Replaces the reference's module-private helper, split at its
+ * objective evaluations. */
+int pk_wolfe_phase(int phase, int dtype_bytes, void* const* arrays, int M, int N, int ls_iter, double c1, double c2,
+                   double tol_change, int flag_arg, void* stream);
+
+/* After a search (:621-624, :632): rows with in_ls take x += t d and the
+ * search's loss and gradient; evals are adjusted so the history phase leaves
+ * func_evals += ls_evals for them and += 0 for the rest. */
+int pk_wolfe_apply(int dtype_bytes, void* x, void* g, void* loss, int* evals, const void* d, const void* t,
+                   const void* f_new, const void* g_new, const int* in_ls, const int* ls_evals, int M, int N,
+                   void* stream);
+
 typedef struct PkRelaxParams {
     int max_iter;             /* n_iterations */
     int history;              /* history_size, 1..64 */

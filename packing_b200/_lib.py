@@ -101,6 +101,8 @@ SIGNATURES = {
     "pk_diversity_costs": [_P, _P, _I, _I, _I, _I, _P, _P],
     "pk_diversity_shortcut": [_P, _P, _I, _I, _I, _F, _F, _I, _P, _P],
     "pk_lbfgs_phase": [_I, _I, _P, _I, _I, _I, _I, _D, _D, _D, _D, _I, _I, _P],
+    "pk_wolfe_phase": [_I, _I, _P, _I, _I, _I, _D, _D, _D, _I, _P],
+    "pk_wolfe_apply": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P],
     "pk_relax": [_P, _P, _P, _P, _I, _I, ctypes.POINTER(PkCostSpec), ctypes.POINTER(PkRelaxParams), _P, _P, _P,
                  _P, _P, _P],
     "pk_relax_workspace_floats": [_P, _I, _I, _I],

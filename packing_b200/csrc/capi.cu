@@ -8,6 +8,7 @@
 #include "lap.cuh"
 #include "lbfgs.cuh"
 #include "validate.cuh"
+#include "wolfe.cuh"
 
 extern "C" int pk_version(void) { return 1; }
 

@@ -181,6 +181,10 @@ __device__ __forceinline__ float pk_radd(float a, float b) { return __fadd_rn(a,
 __device__ __forceinline__ double pk_radd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float pk_rsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ double pk_rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float pk_rdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double pk_rdiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float pk_rsqrt(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ double pk_rsqrt(double a) { return __dsqrt_rn(a); }
 
 // Order-fixed vector reductions.  Element k belongs to group k / 128 and
 // lane k % 32; thread (warp w, lane l) OWNS the elements of the groups

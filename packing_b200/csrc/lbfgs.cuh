@@ -574,12 +574,12 @@ __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restric
     if (!PERSISTENT) {
         pk_relax_instance<MODE>(order ? order[blockIdx.x] : blockIdx.x, xyt_in, h_in, offsets, E, n_max, spec, prm,
                                 xyt_out, h_out, loss_out, iters_out, work, cap_near, cap_items, pk_smem);
-        return;
-    }
-    for (int k = blockIdx.x; k < E; k += gridDim.x) {
-        pk_relax_instance<MODE>(order ? order[k] : k, xyt_in, h_in, offsets, E, n_max, spec, prm, xyt_out, h_out,
-                                loss_out, iters_out, work, cap_near, cap_items, pk_smem);
-        __syncthreads();   // shared state is reused by the next instance
+    } else {
+        for (int k = blockIdx.x; k < E; k += gridDim.x) {
+            pk_relax_instance<MODE>(order ? order[k] : k, xyt_in, h_in, offsets, E, n_max, spec, prm, xyt_out, h_out,
+                                    loss_out, iters_out, work, cap_near, cap_items, pk_smem);
+            __syncthreads();   // shared state is reused by the next instance
+        }
     }
 }
 

@@ -113,10 +113,87 @@ def lbfgs_fixture(ref_root):
              x0_pack=x0p, x_pack=xp.numpy(), n_pack=n)
 
 
+def wolfe_problems():
+    """The strong-Wolfe fixture's problems.  The search evaluates row
+    subsets, so every objective is the same function on every row: a convex
+    quadratic (one A, b), an extended Rosenbrock function and the packing
+    cost of the oracle."""
+    rng = np.random.default_rng(11)
+    N = 12
+    A = rng.normal(size=(N, N))
+    A = A @ A.T + N * np.eye(N)
+    bvec = rng.normal(size=N)
+    x0q = rng.normal(size=(4, N)) * 2.0
+    x0r = rng.uniform(-2.0, 2.0, size=(6, 6))
+    n, E = 6, 3
+    xyt = np.stack([O.place_random(n, 1.3 * np.sqrt(n * 0.2456875), 40 + s) for s in range(E)])
+    x0p = np.concatenate([xyt.reshape(E, -1), np.tile([[1.6, 0.0, 0.0]], (E, 1))], axis=1)
+    return dict(A=A, b=bvec, x0_quad=x0q, x0_rosen=x0r, x0_pack=x0p, n_pack=n)
+
+
+def quad_np(A, bvec, x):
+    Ax = x @ A.T
+    return 0.5 * (x * Ax).sum(1) - x @ bvec, Ax - bvec
+
+
+def rosenbrock_np(x):
+    a, b = x[:, 0::2], x[:, 1::2]
+    f = (100.0 * (b - a ** 2) ** 2 + (1.0 - a) ** 2).sum(1)
+    g = np.zeros_like(x)
+    g[:, 0::2] = -400.0 * a * (b - a ** 2) - 2.0 * (1.0 - a)
+    g[:, 1::2] = 200.0 * (b - a ** 2)
+    return f, g
+
+
+def pack_np(n, x):
+    E = len(x)
+    c, g, gh = O.compound_cost(x[:, :3 * n].reshape(E, n, 3), x[:, 3 * n:], w_area=1e-2, fixed_h=True)
+    return c, np.concatenate([g.reshape(E, -1), gh], 1)
+
+
+WOLFE_CASES = [
+    ("quad_free", "quad", dict(max_iter=12, history_size=5, max_step=None, tolerance_grad=0, tolerance_change=0)),
+    ("quad_clamped", "quad", dict(max_iter=12, history_size=3, max_step=0.3, tolerance_grad=0, tolerance_change=0,
+                                  lr=0.8)),
+    ("rosen", "rosen", dict(max_iter=40, history_size=5, max_step=None, tolerance_grad=1e-10,
+                            tolerance_change=1e-12)),
+    ("pack", "pack", dict(max_iter=15, history_size=3, max_step=0.05, tolerance_grad=0, tolerance_change=0)),
+]
+
+
+def wolfe_fixture(ref_root):
+    """Final iterates and the sequence of objective calls (rows, is_main) of
+    the reference's lbfgs with line_search_fn='strong_wolfe' (CPU torch,
+    float64) on the problems above."""
+    sys.path.insert(0, os.path.join(ref_root, "core"))
+    import torch
+    import lbfgs_torch_parallel as R
+
+    P = wolfe_problems()
+    A, bvec, n = P["A"], P["b"], int(P["n_pack"])
+    fns = {"quad": lambda x: quad_np(A, bvec, x), "rosen": rosenbrock_np, "pack": lambda x: pack_np(n, x)}
+    out = dict(P)
+    for name, kind, kw in WOLFE_CASES:
+        x0 = P["x0_" + kind]
+        log = []
+
+        def f_t(x, is_main, kind=kind, log=log):
+            log.append((x.shape[0], int(bool(is_main))))
+            c, g = fns[kind](x.numpy())
+            return torch.from_numpy(np.asarray(c)), torch.from_numpy(np.asarray(g))
+
+        xt = torch.from_numpy(x0.copy())
+        R.lbfgs(f_t, xt, line_search_fn="strong_wolfe", **kw)
+        out[f"x_{name}"] = xt.numpy()
+        out[f"calls_{name}"] = np.array(log, dtype=np.int64).reshape(-1, 2)
+    np.savez(os.path.join(HERE, "lbfgs_wolfe_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     with open(os.path.join(HERE, "cost_cases.json"), "w") as f:
         json.dump(cost_cases(), f, indent=1)
     ref = sys.argv[1] if len(sys.argv) > 1 else None
     if ref:
         lbfgs_fixture(ref)
+        wolfe_fixture(ref)
     print("golden fixtures written to", HERE)
