@@ -149,6 +149,23 @@ FLOPS_PER_PIECE_PAIR = 424
 FLOPS_PER_HIST_ELEM = 4
 FLOPS_PER_ITER_ELEM = 12
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one relaxation
+# launch, from a one-pass ncu capture of that launch, per (E, n, iterations,
+# history); other configurations report null.  Almost all of it is the final
+# write-back of the L-BFGS history (2 m (3n + 3) floats per packing).
+TRAFFIC_BYTES = {(4096, 200, 200, 10): 344.6e6}
+HBM_FALLBACK_GBPS = 6650.0
+
+
+def measured_hbm_gbps():
+    """The measured copy bandwidth of this pool's B200s (MEASURED_PEAKS.json
+    beside this file), else the earlier measurement on the pool."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return HBM_FALLBACK_GBPS, "fallback"
+
 
 def run_ours(args, rank, world, dev):
     import torch
@@ -173,7 +190,9 @@ def run_ours(args, rank, world, dev):
     spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
     # launch shape (threads per packing, persistent grid) from the autotuner;
     # tuning runs before the warm-up and outside the timed region
-    prm = tuned(RelaxParams(n_iterations=iters, history_size=hist, max_step=0.01, final_eval=False), n, spec, dev)
+    prm = RelaxParams(n_iterations=iters, history_size=hist, max_step=0.01, final_eval=False)
+    if not args.no_tune:
+        prm = tuned(prm, n, spec, dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, device=dev)   # > 126 MB L2
     st = torch.cuda.current_stream(dev)
 
@@ -280,9 +299,15 @@ def run_ours(args, rank, world, dev):
              + cnt[5] * FLOPS_PER_HIST_ELEM + cnt[4] * N * FLOPS_PER_ITER_ELEM)
     peak = fp32_peak_tflops(torch, L, dev)
     achieved = flops / kernel_s / 1e12
+    traffic = TRAFFIC_BYTES.get((E, n, iters, hist))
+    hbm_peak, hbm_src = measured_hbm_gbps()
     out["roofline"] = {"bound": "fp32_simt", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                       "frac": achieved / peak, "traffic": None,
-                       "peak_source": "measured FP32 FMA probe on this GPU (pk_fma_probe)",
+                       "frac": achieved / peak, "traffic": traffic,
+                       "peak_source": "measured FP32 FMA probe on this GPU (pk_fma_probe); no tensor-core work: "
+                                      "pairwise clipping is not a contraction",
+                       "hbm": None if traffic is None else {
+                           "achieved_GBps": traffic / kernel_s / 1e9, "peak_GBps": hbm_peak,
+                           "frac": traffic / kernel_s / 1e9 / hbm_peak, "peak_source": hbm_src},
                        "work": {"pairs_enumerated": cnt[0], "near_pairs": cnt[1], "piece_pairs": cnt[2],
                                 "cost_evals": cnt[3], "iterations": cnt[4]}}
 
@@ -507,6 +532,42 @@ def measure_ga_step(args, dev):
             "generations_per_s": 1e3 / step_ms, "relax_iterations": args.ga_iters}
 
 
+def run_cost_case(args, dev):
+    """The compound cost kernel alone (boundary + overlap area and their
+    gradients) on E packings of n trees: --steps launches at the seeded
+    initial poses, then --steps at the poses after --iters iterations of the
+    fused relaxation.  A profiling case, not a benchmark metric."""
+    import torch
+
+    from packing_b200 import _lib
+    from packing_b200.cost import CostSpec, compound_cost
+    from packing_b200.relax import RelaxParams, relax
+    _lib.ensure_init(dev)
+    E, n = args.E, args.n
+    xyt_np, h_np = workload(E, n, seed=0)
+    xyt = torch.from_numpy(xyt_np).to(dev)
+    h = torch.from_numpy(h_np).to(dev)
+    spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
+    xr, _, _, _ = relax(xyt, h, spec, RelaxParams(n_iterations=args.iters, history_size=args.history,
+                                                  max_step=0.01, final_eval=False))
+    c = torch.empty(E, device=dev)
+    g = torch.empty_like(xyt)
+    gh = torch.empty_like(h)
+    out = {"case": "cost", "E": E, "n": n}
+    for name, x in (("initial", xyt), ("relaxed", xr)):
+        for _ in range(args.warmup):
+            compound_cost(x, h, spec, out_cost=c, out_grad=g, out_grad_h=gh)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            compound_cost(x, h, spec, out_cost=c, out_grad=g, out_grad_h=gh)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        out[f"ms_{name}"] = e0.elapsed_time(e1) / args.steps
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -558,6 +619,11 @@ def main():
     ap.add_argument("--ga-P", dest="ga_P", type=int, default=2048)
     ap.add_argument("--ga-iters", dest="ga_iters", type=int, default=100)
     ap.add_argument("--quick", action="store_true", help="headline timing only")
+    ap.add_argument("--no-tune", dest="no_tune", action="store_true",
+                    help="default launch shape instead of the autotuned one (profiling captures)")
+    ap.add_argument("--case", default="relax", choices=["relax", "cost"],
+                    help="relax: the headline; cost: the compound cost kernel alone on E packings, at the "
+                         "initial poses and after --iters iterations of relaxation (profiling captures)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -576,7 +642,7 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=dev)
-    out = run_ours(args, rank, world, dev)
+    out = run_cost_case(args, dev) if args.case == "cost" else run_ours(args, rank, world, dev)
     if rank == 0:
         print(json.dumps(out))
     if world > 1:
