@@ -112,6 +112,15 @@ int pk_cost(const float* xyt, const int* offsets, int E, int n_uniform, const fl
 int pk_overlap(const float* xyt, int E, int n, int use_separation, float* cost, float* grad,
                void* stream);
 
+/* Periodic form of pk_overlap (overlap_multi_ensemble with crystal_axes,
+ * pack_cuda.py:1040-1183; kernel :254-464 with ENABLE_CRYSTAL_AXES): every
+ * tree against every tree's images under cx A + cy B, |cx|, |cy| <=
+ * n_periodic, crystal_axes (E, 4) = [ax, ay, bx, by] float32.  Images of a
+ * tree itself count half (all of it with only_self, which keeps only those)
+ * and add no gradient, as in the reference.  grad nullable. */
+int pk_overlap_crystal(const float* xyt, int E, int n, int use_separation, const float* crystal_axes, int only_self,
+                       int n_periodic, float* cost, float* grad, void* stream);
+
 /* pack_cuda.boundary_distance_multi_ensemble (pack_cuda.py:1186-1295). */
 int pk_boundary(const float* xyt, const float* h, int E, int n, float* cost, float* grad,
                 float* grad_h, void* stream);

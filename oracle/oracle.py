@@ -52,6 +52,7 @@ def lib():
         L.oracle_geometry.argtypes = [P, P, P, P]
         L.oracle_pair_cost.argtypes = [P, i, i, i, P, P, P]
         L.oracle_boundary.argtypes = [P, P, i, i, P, P, P]
+        L.oracle_pair_cost_crystal.argtypes = [P, i, i, i, P, i, i, P, P]
         L.oracle_lut_cost.argtypes = [P, P, i, P, i, i, i, P, i, ctypes.c_double, P, P]
         L.oracle_hungarian.argtypes = [P, i, i, P, P, P]
         L.oracle_diversity_shortcut.argtypes = [P, P, i, i, i, ctypes.c_float, ctypes.c_float, i, P]
@@ -93,6 +94,36 @@ def pair_cost(xyt, use_separation=False, grad=True, counters=False):
     lib().oracle_pair_cost(_p(xyt), E, n, int(bool(use_separation)), _p(cost), _p(g), _p(cnt))
     out = (cost, g)
     return out + (cnt,) if counters else out
+
+
+def pair_cost_crystal(xyt, crystal_axes, use_separation=False, only_self_interactions=False, n_periodic=2,
+                      grad=True):
+    """Periodic overlap area (or sum of sep^2) with the ref-pose gradient,
+    ``pack_cuda.py:254-546`` with crystal axes (E, 4) = [ax, ay, bx, by]."""
+    xyt = np.ascontiguousarray(xyt, dtype=np.float64)
+    axes = np.ascontiguousarray(crystal_axes, dtype=np.float64).reshape(-1, 4)
+    E, n, _ = xyt.shape
+    cost = np.zeros(E)
+    g = np.zeros_like(xyt) if grad else None
+    lib().oracle_pair_cost_crystal(_p(xyt), E, n, int(bool(use_separation)), _p(axes),
+                                   int(bool(only_self_interactions)), int(n_periodic), _p(cost), _p(g))
+    return cost, g
+
+
+def lattice_axes(kind, h, aspect=None, angle=None):
+    """Crystal axes [ax, ay, bx, by] of the reference's lattice collections
+    (kaggle_support.py:1690-1708 Lattice, 1817-1835 LatticeRectangle,
+    1876-1885 LatticeFixed with angle pi/2 unless given, :1935-1938)."""
+    h = np.asarray(h, np.float64)
+    if kind == "lattice":
+        return np.array([h[0], 0.0, h[1] * np.cos(h[2]), h[1] * np.sin(h[2])])
+    if kind == "rectangle":
+        return np.array([h[0], 0.0, 0.0, h[1]])
+    if kind == "fixed":
+        ang = np.pi / 2 if angle is None else angle
+        b = h[0] * aspect
+        return np.array([h[0], 0.0, b * np.cos(ang), b * np.sin(ang)])
+    raise ValueError(kind)
 
 
 def boundary(xyt, h):

@@ -442,6 +442,93 @@ void oracle_pair_cost(const double* xyt, int E, int n, int use_sep, double* cost
                       grad ? grad + (size_t)e * n * 3 : NULL, counters ? counters + 2 * e : NULL);
 }
 
+/* Periodic form of pair_cost_one: overlap_ref_with_list_piece with
+ * use_crystal (pack_cuda.py:254-393, 332-364) and overlap_list_total
+ * (:404-464).  For every ref tree i and every tree j (j == i included) the
+ * images j + cx A + cy B, cx, cy in [-N_periodic, N_periodic], are tested,
+ * except j == i at the origin cell; the centre cutoff is applied to the image
+ * (process_tree_pair_piece :159-168).  The ref gradient is accumulated except
+ * for images of the ref tree itself (:350-351).  only_self keeps only j == i
+ * and the total is not halved (:455-460); otherwise it is halved. */
+static void pair_cost_crystal_one(const double* xyt, int n, int use_sep, const double* axes, int only_self,
+                                  int np_, double* cost, double* grad)
+{
+    double total = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double rx = xyt[3 * i], ry = xyt[3 * i + 1], rt = xyt[3 * i + 2];
+        double c = cos(rt), s = sin(rt);
+        double gi[3] = {0, 0, 0};
+        double tsum = 0.0;
+        for (int pi = 0; pi < MAXP; ++pi) {
+            d2 rp[MAXV];
+            double rbb[4];
+            piece_world(rx, ry, c, s, pi, rp, rbb);
+            int n1 = g_piece_nv[pi];
+            for (int j = 0; j < n; ++j) {
+                int self = j == i;
+                if (only_self && !self) continue;
+                for (int cx = -np_; cx <= np_; ++cx) {
+                    for (int cy = -np_; cy <= np_; ++cy) {
+                        if (self && cx == 0 && cy == 0) continue;
+                        double ox = xyt[3 * j] + cx * axes[0] + cy * axes[2];
+                        double oy = xyt[3 * j + 1] + cx * axes[1] + cy * axes[3];
+                        double ot = xyt[3 * j + 2];
+                        double dx = ox - rx, dy = oy - ry;
+                        if (dx * dx + dy * dy > g_cutoff_sq) continue;
+                        int want_grad = grad && !self;
+                        double oc = cos(ot), os = sin(ot);
+                        for (int pj = 0; pj < MAXP; ++pj) {
+                            d2 op[MAXV];
+                            double obb[4];
+                            piece_world(ox, oy, oc, os, pj, op, obb);
+                            if (rbb[1] < obb[0] || obb[1] < rbb[0] || rbb[3] < obb[2] || obb[3] < rbb[2]) continue;
+                            if (!use_sep) {
+                                d2 dsub[MAXV];
+                                double a = convex_isect_area(rp, n1, op, g_piece_nv[pj], want_grad ? dsub : NULL);
+                                tsum += a;
+                                if (want_grad && a != 0.0) {
+                                    for (int v = 0; v < n1; ++v) {
+                                        double lx = g_piece[pi][v].x, ly = g_piece[pi][v].y;
+                                        gi[0] += dsub[v].x;
+                                        gi[1] += dsub[v].y;
+                                        gi[2] += dsub[v].x * (-s * lx - c * ly);
+                                        gi[2] += dsub[v].y * (c * lx - s * ly);
+                                    }
+                                }
+                            } else {
+                                double sp, gx, gy, gt;
+                                sat_sep(g_piece[pi], n1, op, g_piece_nv[pj], rx, ry, c, s, &sp, &gx, &gy, &gt);
+                                if (sp > 0.0) {
+                                    tsum += sp * sp;
+                                    if (want_grad) {
+                                        gi[0] += 2.0 * sp * gx;
+                                        gi[1] += 2.0 * sp * gy;
+                                        gi[2] += 2.0 * sp * gt;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        total += only_self ? tsum : tsum / 2.0;
+        if (grad) { grad[3 * i] = gi[0]; grad[3 * i + 1] = gi[1]; grad[3 * i + 2] = gi[2]; }
+    }
+    *cost = total;
+}
+
+/* overlap_multi_ensemble with crystal_axes (E, 4) = [ax, ay, bx, by],
+ * pack_cuda.py:1040-1183. */
+void oracle_pair_cost_crystal(const double* xyt, int E, int n, int use_sep, const double* axes, int only_self,
+                              int n_periodic, double* cost, double* grad)
+{
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int e = 0; e < E; ++e)
+        pair_cost_crystal_one(xyt + (size_t)e * n * 3, n, use_sep, axes + 4 * (size_t)e, only_self, n_periodic,
+                              cost + e, grad ? grad + (size_t)e * n * 3 : NULL);
+}
+
 /* boundary_distance_tree / multi_boundary_distance_list_total,
  * pack_cuda.py:550-757 */
 void oracle_boundary(const double* xyt, const double* h, int E, int n, double* cost,

@@ -93,6 +93,7 @@ SIGNATURES = {
     "pk_last_error": [],
     "pk_cost": [_P, _P, _I, _I, _P, ctypes.POINTER(PkCostSpec), _P, _P, _P, _P],
     "pk_overlap": [_P, _I, _I, _I, _P, _P, _P],
+    "pk_overlap_crystal": [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P],
     "pk_boundary": [_P, _P, _I, _I, _P, _P, _P, _P],
     "pk_overlap_lut": [_P, _P, _I, _I, ctypes.POINTER(PkLut), _P, _P, _P],
     "pk_lut_build": [_P, _I, _P, _I, _P, _I, _I, _P, _P],

@@ -9,6 +9,7 @@
 #include "lbfgs.cuh"
 #include "validate.cuh"
 #include "wolfe.cuh"
+#include "crystal.cuh"
 
 extern "C" int pk_version(void) { return 1; }
 

@@ -8,9 +8,13 @@ overwritten, the functions return ``None``.  Arguments are validated on
 every call (the reference does it only at ``debugging_mode >= 2``) and raise
 ``ValueError`` like the reference's checks.
 
-Not provided (outside the non-periodic hot path): ``crystal_axes`` /
-``only_self_interactions`` periodic images (``pack_cuda.py:332-364``) and
-distinct ``xyt1``/``xyt2`` arrays; both raise ``NotImplementedError``.
+Periodic images (``crystal_axes`` (E, 4) = [ax, ay, bx, by],
+``only_self_interactions``, ``N_periodic``; ``pack_cuda.py:332-364``) run in
+a kernel of their own (``pk_overlap_crystal``) with the reference's rules:
+images of a tree itself count half and carry no gradient, ``only_self``
+keeps only those at full weight, and with ``only_self_interactions`` but no
+axes the result is zero.  Distinct ``xyt1``/``xyt2`` arrays raise
+``NotImplementedError`` (every caller passes one array).
 """
 from __future__ import annotations
 
@@ -35,8 +39,6 @@ def overlap_multi_ensemble(xyt1, xyt2, use_separation, out_cost=None, out_grads=
     penetration depths (``True``) over all tree pairs of each ensemble, and
     optionally its gradient w.r.t. every pose.  Reference:
     ``pack_cuda.py:1040-1183`` (kernel ``multi_overlap_list_total`` :482)."""
-    if crystal_axes is not None or only_self_interactions:
-        raise NotImplementedError("periodic (crystal) images are outside the non-periodic hot path")
     if not isinstance(use_separation, bool) and type(use_separation).__name__ != "bool_":
         raise ValueError("use_separation must be a boolean")
     x1 = _lib.as_tensor(xyt1, "xyt1")
@@ -56,12 +58,29 @@ def overlap_multi_ensemble(xyt1, xyt2, use_separation, out_cost=None, out_grads=
     if out_grads is not None:
         g = _lib.as_tensor(out_grads, "out_grads")
         _lib.check_f32(g, "out_grads", (E, n, 3))
+    ax = None
+    if crystal_axes is not None:
+        ax = _lib.as_tensor(crystal_axes, "crystal_axes")
+        _lib.check_f32(ax, "crystal_axes", (E, 4))
+        if not isinstance(N_periodic, (int,)) or N_periodic < 0:
+            raise ValueError("N_periodic must be a non-negative int")
     if E == 0:
+        return
+    if ax is None and only_self_interactions:
+        # no periodic images: no self interactions (pack_cuda.py:1061-1062)
+        c.zero_()
+        if g is not None:
+            g.zero_()
         return
     _lib.ensure_init(x1.device)
     with torch.cuda.device(x1.device):
-        rc = _lib.load().pk_overlap(_lib.ptr(x1), E, n, int(bool(use_separation)), _lib.ptr(c), _lib.ptr(g),
-                                    ctypes.c_void_p(_lib.stream_handle(stream, x1.device)))
+        sh = ctypes.c_void_p(_lib.stream_handle(stream, x1.device))
+        if ax is None:
+            rc = _lib.load().pk_overlap(_lib.ptr(x1), E, n, int(bool(use_separation)), _lib.ptr(c), _lib.ptr(g), sh)
+        else:
+            rc = _lib.load().pk_overlap_crystal(_lib.ptr(x1), E, n, int(bool(use_separation)), _lib.ptr(ax),
+                                                int(bool(only_self_interactions)), int(N_periodic), _lib.ptr(c),
+                                                _lib.ptr(g), sh)
     _lib.check(rc, "overlap_multi_ensemble")
 
 

@@ -219,5 +219,8 @@ def test_argument_errors(cuda):
         pack_cuda.overlap_multi_ensemble(x, x, False, out_cost=torch.zeros(3, device=cuda))
     with pytest.raises(NotImplementedError):
         pack_cuda.overlap_multi_ensemble(x, x.clone(), False, out_cost=c)
-    with pytest.raises(NotImplementedError):
-        pack_cuda.overlap_multi_ensemble(x, x, False, out_cost=c, crystal_axes=torch.zeros(2, 4, device=cuda))
+    with pytest.raises(ValueError):   # crystal axes must be (E, 4)
+        pack_cuda.overlap_multi_ensemble(x, x, False, out_cost=c, crystal_axes=torch.zeros(3, 4, device=cuda))
+    with pytest.raises(ValueError):
+        pack_cuda.overlap_multi_ensemble(x, x, False, out_cost=c, crystal_axes=torch.zeros(2, 4, device=cuda),
+                                         N_periodic=-1)

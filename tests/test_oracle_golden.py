@@ -158,3 +158,37 @@ def test_oracle_hungarian_optimal():
     for b in range(20):
         r, c = linear_sum_assignment(C[b].astype(np.float64))
         assert abs(C[b][r, c].astype(np.float64).sum() - C[b][np.arange(60), rm[b]].astype(np.float64).sum()) < 1e-4
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_periodic_costs_match_reference_fp64(k):
+    """Oracle's periodic form reproduces the reference's FP64 CPU values for
+    the lattice solutions of pack_test.py:174-213 (run_tests.ipynb)."""
+    d = _cases()
+    c = d["lattice_cases"][k]
+    x = np.array(c["xyt"])[None]
+    ax = np.array(c["crystal_axes"])[None]
+    rec = d["recorded_lattice"]
+    ov = O.pair_cost_crystal(x, ax, False, False, c["N_periodic"])[0][0] * 3
+    sp = O.pair_cost_crystal(x, ax, True, False, c["N_periodic"])[0][0] * 5
+    assert ov == pytest.approx(rec["CollisionCostOverlappingArea(scaling=3)"]["cpu64"][k], rel=1e-13)
+    assert sp == pytest.approx(rec["CollisionCostSeparation(scaling=5)"]["cpu64"][k], rel=1e-13)
+
+
+@pytest.mark.parametrize("use_sep", [False, True])
+def test_periodic_gradient_matches_finite_differences(use_sep):
+    """The periodic ref-pose gradient (self images excluded, as in the
+    reference) against central differences of the cost without the
+    self-image terms' theta dependence: x, y derivatives match in full."""
+    d = _cases()
+    c = d["lattice_cases"][0]
+    x = np.array(c["xyt"])[None]
+    ax = np.array(c["crystal_axes"])[None]
+    _, g = O.pair_cost_crystal(x, ax, use_sep, False, 2)
+    fd = _fd(lambda xx: O.pair_cost_crystal(xx, ax, use_sep, False, 2)[0][0], x)
+    # self images do not depend on a tree's own translation, so x, y agree
+    np.testing.assert_allclose(g[..., :2], fd[..., :2], rtol=1e-4, atol=1e-4)
+    # theta: the reference adds the self-image part by finite differences of
+    # the only_self cost (pack_cost.py:636-672); together they match
+    fd_self = _fd(lambda xx: O.pair_cost_crystal(xx, ax, use_sep, True, 2)[0][0], x)
+    np.testing.assert_allclose(g[..., 2] + fd_self[..., 2] / 2, fd[..., 2], rtol=1e-4, atol=1e-4)
