@@ -340,7 +340,8 @@ def run_ours(args, rank, world, dev):
 
     # ---- secondary configurations: serving, ragged LUT, GA generation ----
     if not args.skip_extra:
-        for name, fn in [("serve", measure_serve), ("ragged_lut", measure_ragged_lut), ("ga_step", measure_ga_step)]:
+        for name, fn in [("serve", measure_serve), ("ragged_lut", measure_ragged_lut), ("ga_step", measure_ga_step),
+                         ("legalize", measure_legalize)]:
             try:
                 out[name] = fn(args, dev)
             except Exception as exc:   # reported, the headline stands
@@ -532,6 +533,39 @@ def measure_ga_step(args, dev):
             "generations_per_s": 1e3 / step_ms, "relax_iterations": args.ga_iters}
 
 
+def measure_legalize(args, dev):
+    """Acceptance of relaxed packings (pack_io.py:28-112): a sample of n = 200
+    packings relaxed by the area cost at a looser side, then snapped and
+    legalised with the reference's schedule; acceptance is the FP64 legality
+    check on the GPU (tests/test_legalize_gpu.py holds it against the
+    oracle's independent check)."""
+    import torch
+
+    from packing_b200.cost import CostSpec
+    from packing_b200.legalize import legalize
+    from packing_b200.relax import RelaxParams, relax
+    E, n = args.legal_E, args.n
+    xyt_np, _ = workload(E, n, seed=31)
+    x = torch.from_numpy(xyt_np).to(dev)
+    h = torch.zeros((E, 3), device=dev)
+    h[:, 0] = float(1.3 * np.sqrt(n * TREE_AREA) + 1.5)
+    xr, hr, _, _ = relax(x, h, CostSpec(pair="area", w_area=1e-2, fixed_h=True),
+                         RelaxParams(n_iterations=400, history_size=args.history, max_step=0.01))
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    r = legalize(xr, hr)
+    torch.cuda.synchronize(dev)
+    dt = time.perf_counter() - t0
+    legal = r.legal.cpu().numpy()
+    side = r.side.cpu().numpy()
+    return {"packings": E, "n": n, "accepted_fp64": int(legal.sum()),
+            "side_mean_accepted": float(side[legal].mean()) if legal.any() else None,
+            "rounds_max": int(r.rounds.max()), "seconds": dt,
+            "schedule": "snap, then up to 20 rounds: area weight 1e-2 halved, max_step 1e-4 x sqrt(1/2)^k, "
+                        "20000 then 2000 iterations, history 10, until boundary + separation < 1e-10; "
+                        "FP64 check; one retry with tolerance_rel_change 0"}
+
+
 def run_cost_case(args, dev):
     """The compound cost kernel alone (boundary + overlap area and their
     gradients) on E packings of n trees: --steps launches at the seeded
@@ -618,6 +652,7 @@ def main():
     ap.add_argument("--lut-E", dest="lut_E", type=int, default=8192)
     ap.add_argument("--ga-P", dest="ga_P", type=int, default=2048)
     ap.add_argument("--ga-iters", dest="ga_iters", type=int, default=100)
+    ap.add_argument("--legal-E", dest="legal_E", type=int, default=64)
     ap.add_argument("--quick", action="store_true", help="headline timing only")
     ap.add_argument("--no-tune", dest="no_tune", action="store_true",
                     help="default launch shape instead of the autotuned one (profiling captures)")

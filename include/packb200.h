@@ -313,6 +313,12 @@ int pk_relax_noalloc(const float* xyt_in, const float* h_in, int E, int n, const
                      const PkRelaxParams* params, float* xyt_out, float* h_out, float* loss_out, int* iters_out,
                      void* stream);
 
+/* SolutionCollectionSquare.snap (kaggle_support.py:824-879): each packing's
+ * trees re-centred on the bounding box of their (search-tree) vertices and h
+ * = (min(side, h_in[0]), 0, 0), side = max(width, height); h_in nullable
+ * (then h = (side, 0, 0)).  xyt_out may alias xyt_in. */
+int pk_snap(const float* xyt_in, const float* h_in, int E, int n, float* xyt_out, float* h_out, void* stream);
+
 /* Floats of work needed by pk_relax: sizes_host (E,) host int32 tree counts
  * for a ragged batch, or NULL and n_uniform for a uniform one. */
 size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, int history);

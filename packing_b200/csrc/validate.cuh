@@ -128,3 +128,59 @@ extern "C" int pk_validate_fp64(const void* xyt, int dtype_bytes, int E, int n, 
     if (err != cudaSuccess) return pk_cuda_check(err, "pk_validate_fp64 attribute");
     return pk_cuda_check(cudaGetLastError(), "pk_validate_fp64 launch");
 }
+
+// SolutionCollectionSquare.snap (kaggle_support.py:824-879), FP32 as the
+// reference runs it: the bounding box of every search-tree vertex (each
+// rounded as cos lx - sin ly, then + x), the trees re-centred on it, side =
+// max(width, height) and h = (min(side, h0), 0, 0) (h0 = +inf without h_in).
+__global__ void pk_snap_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in, int E, int n,
+                               float* __restrict__ xyt_out, float* __restrict__ h_out)
+{
+    __shared__ float red[4 * 32];
+    const int e = blockIdx.x;
+    if (e >= E) return;
+    const float* X = xyt_in + (size_t)e * n * 3;
+    float4 bb = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, -3.4e38f);   // -min x, max x, -min y, max y
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const float x = X[3 * t], y = X[3 * t + 1], th = X[3 * t + 2];
+        float s, c;
+        sincosf(th, &s, &c);
+        for (int v = 0; v < c_geom.n_tree; ++v) {
+            const float2 l = c_geom.tree[v];
+            const float vx = __fadd_rn(__fsub_rn(__fmul_rn(c, l.x), __fmul_rn(s, l.y)), x);
+            const float vy = __fadd_rn(__fadd_rn(__fmul_rn(s, l.x), __fmul_rn(c, l.y)), y);
+            bb.x = fmaxf(bb.x, -vx); bb.y = fmaxf(bb.y, vx);
+            bb.z = fmaxf(bb.z, -vy); bb.w = fmaxf(bb.w, vy);
+        }
+    }
+    bb = pk_block_max4(bb, red);
+    const float x0 = -bb.x, x1 = bb.y, y0 = -bb.z, y1 = bb.w;
+    const float xc = (x0 + x1) / 2.0f, yc = (y0 + y1) / 2.0f;
+    const float size = fmaxf(x1 - x0, y1 - y0);
+    float* Xo = xyt_out + (size_t)e * n * 3;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const float x = X[3 * t], y = X[3 * t + 1], th = X[3 * t + 2];
+        Xo[3 * t] = x - xc;
+        Xo[3 * t + 1] = y - yc;
+        Xo[3 * t + 2] = th;
+    }
+    if (threadIdx.x == 0) {
+        h_out[3 * e] = h_in ? fminf(size, h_in[3 * e]) : size;
+        h_out[3 * e + 1] = 0.f;
+        h_out[3 * e + 2] = 0.f;
+    }
+}
+
+extern "C" int pk_snap(const float* xyt_in, const float* h_in, int E, int n, float* xyt_out, float* h_out,
+                       void* stream)
+{
+    int rc = pk_check_init();
+    if (rc) return rc;
+    if (E < 0 || n < 1) return pk_fail(PK_EINVAL, "pk_snap: needs E >= 0 and n >= 1%s");
+    if (n > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_snap: more than 1024 trees%s");
+    if (E == 0) return PK_OK;
+    if (!xyt_in || !xyt_out || !h_out) return pk_fail(PK_EINVAL, "pk_snap: NULL pointer%s");
+    const int T = n <= 64 ? 64 : (n <= 128 ? 128 : 256);
+    pk_snap_kernel<<<E, T, 0, (cudaStream_t)stream>>>(xyt_in, h_in, E, n, xyt_out, h_out);
+    return pk_cuda_check(cudaGetLastError(), "pk_snap launch");
+}
