@@ -96,6 +96,10 @@ typedef struct PkCostSpec {
     float w_area;         /* AreaCost of a square: h0^2 (kaggle_support.py:803-816) */
     int fixed_h;
     PkLut lut;            /* used when pair_mode == PK_PAIR_LUT */
+    int symmetry;         /* 0 or 1: xyt holds every tree; 2 / 4: xyt holds the genotype of a
+                             180 / 90 degree symmetric packing (SolutionCollectionSquareSymmetric180
+                             / 90, kaggle_support.py:1272-1393 / 1039-1195): the cost is that of the
+                             2 n / 4 n image trees and the gradient is the genotype's */
 } PkCostSpec;
 
 /* Compound cost over a uniform (offsets == NULL, all n_uniform trees) or

@@ -56,6 +56,7 @@ class PkCostSpec(ctypes.Structure):
         ("w_area", ctypes.c_float),
         ("fixed_h", ctypes.c_int),
         ("lut", PkLut),
+        ("symmetry", ctypes.c_int),
     ]
 
 

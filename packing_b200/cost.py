@@ -27,6 +27,7 @@ class CostSpec:
     w_area: float = 1e-2
     fixed_h: bool = True
     lut: object = None
+    symmetry: int = 1   # 1: every tree given; 2 / 4: genotype of a 180 / 90 degree symmetric packing
 
     def to_c(self) -> _lib.PkCostSpec:
         s = _lib.PkCostSpec()
@@ -39,6 +40,9 @@ class CostSpec:
         s.w_boundary = float(self.w_boundary)
         s.w_area = float(self.w_area)
         s.fixed_h = int(bool(self.fixed_h))
+        if self.symmetry not in (1, 2, 4):
+            raise ValueError("symmetry must be 1, 2 or 4")
+        s.symmetry = int(self.symmetry)
         if self.pair == "lut":
             if self.lut is None:
                 raise ValueError("pair='lut' needs a LookupTable")

@@ -590,6 +590,28 @@ __device__ __forceinline__ double4 pk_canonical_sum4(int n, const float4* bnd)
     return s;
 }
 
+// Images per genotype tree of a symmetric packing (spec.symmetry): 1, 2
+// (SolutionCollectionSquareSymmetric180, kaggle_support.py:1272-1393) or 4
+// (SolutionCollectionSquareSymmetric90, :1039-1195).
+__host__ __device__ inline int pk_symmetry(const PkCostSpec& spec) { return spec.symmetry > 1 ? spec.symmetry : 1; }
+
+// Pose of phenotype tree t = k ng + g: image k of genotype tree g, as the
+// reference expands it in float32 (the angle offsets are pi / 2, pi and
+// 3 pi / 2 rounded to float32 before the add):
+//   180: (x, y, th), (-x, -y, th + pi)
+//   90:  (x, y, th), (-y, x, th + pi/2), (-x, -y, th + pi), (y, -x, th + 3pi/2)
+__device__ __forceinline__ void pk_image_pose(const float* X, int ng, int sym, int t, float& x, float& y, float& th)
+{
+    const int k = sym == 1 ? 0 : t / ng, g = t - k * ng;
+    const float gx = X[3 * g], gy = X[3 * g + 1], gt = X[3 * g + 2];
+    const float hpi = (float)(3.14159265358979323846 / 2.0), pi = (float)3.14159265358979323846,
+                tpi = (float)(3.0 * 3.14159265358979323846 / 2.0);
+    if (k == 0) { x = gx; y = gy; th = gt; }
+    else if (sym == 2 || k == 2) { x = -gx; y = -gy; th = gt + pi; }
+    else if (k == 1) { x = -gy; y = gx; th = gt + hpi; }
+    else { x = gy; y = -gx; th = gt + tpi; }
+}
+
 struct PkEvalOut {
     double cost;
 };
@@ -598,9 +620,13 @@ struct PkEvalOut {
 // NULL.  G: 3n floats or NULL (written, not accumulated); GH: 3 floats or
 // NULL.  Must be called by every thread of the block.
 template <int MODE>
-__device__ double pk_eval_instance(const float* X, int n, const float* H, const PkCostSpec& spec,
+__device__ double pk_eval_instance(const float* X, int ng, const float* H, const PkCostSpec& spec,
                                    float* G, float* GH, const PkCostSmem& sm)
 {
+    // ng genotype trees in X (3 ng floats); the cost is that of the n
+    // phenotype trees, and G receives the genotype gradient
+    const int sym = pk_symmetry(spec);
+    const int n = sym * ng;
     const int T = blockDim.x;
     const bool do_bnd = spec.w_boundary != 0.f && H != nullptr;
     float half = 0.f, hox = 0.f, hoy = 0.f;
@@ -611,7 +637,8 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
     __syncthreads();
     // ---- phase 0: per tree -------------------------------------------------
     for (int t = threadIdx.x; t < n; t += T) {
-        const float x = X[3 * t], y = X[3 * t + 1], th = X[3 * t + 2];
+        float x, y, th;
+        pk_image_pose(X, ng, sym, t, x, y, th);
         float s, c;
         sincosf(th, &s, &c);
         sm.pose[t] = make_float4(x, y, c, s);
@@ -775,10 +802,24 @@ __device__ double pk_eval_instance(const float* X, int n, const float* H, const 
 
     // ---- phase C: outputs ----------------------------------------------------
     if (G) {
-        for (int t = threadIdx.x; t < n; t += T) {
-            G[3 * t] = (float)((double)sm.acc[3 * t] * PK_FX_INV);
-            G[3 * t + 1] = (float)((double)sm.acc[3 * t + 1] * PK_FX_INV);
-            G[3 * t + 2] = (float)((double)sm.acc[3 * t + 2] * PK_FX_INV);
+        // genotype gradient: the images' gradients through the symmetry's
+        // rotations (backprop_phenotype, kaggle_support.py:1366-1393 and
+        // :1155-1195), combined exactly in fixed point
+        for (int t = threadIdx.x; t < ng; t += T) {
+            const long long* a = sm.acc;
+            long long gx = a[3 * t], gy = a[3 * t + 1], gt = a[3 * t + 2];
+            if (sym == 2) {
+                const int u = 3 * (t + ng);
+                gx -= a[u]; gy -= a[u + 1]; gt += a[u + 2];
+            } else if (sym == 4) {
+                const int u1 = 3 * (t + ng), u2 = 3 * (t + 2 * ng), u3 = 3 * (t + 3 * ng);
+                gx = gx + a[u1 + 1] - a[u2] - a[u3 + 1];
+                gy = gy - a[u1] - a[u2 + 1] + a[u3];
+                gt = gt + a[u1 + 2] + a[u2 + 2] + a[u3 + 2];
+            }
+            G[3 * t] = (float)((double)gx * PK_FX_INV);
+            G[3 * t + 1] = (float)((double)gy * PK_FX_INV);
+            G[3 * t + 2] = (float)((double)gt * PK_FX_INV);
         }
     }
     // one barrier for every total: per-warp pair partials (int64: exact in
@@ -829,7 +870,7 @@ __global__ void __launch_bounds__(256, 3) pk_cost_kernel(const float* __restrict
         if (threadIdx.x == 0) cost[e] = __int_as_float(0x7fc00000);   // NaN marks a bad offset
         return;
     }
-    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap_near, cap_items);
+    PkCostSmem sm = pk_cost_carve(pk_smem, n_max * pk_symmetry(spec), cap_near, cap_items);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
     __syncthreads();
     const double tot = pk_eval_instance<MODE>(xyt + (size_t)base * 3, n, h ? h + 3 * e : nullptr, spec,
@@ -857,7 +898,10 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
     if (!spec) return pk_fail(PK_EINVAL, "pk_cost: spec is NULL%s");
     if (E < 0 || n_max < 0) return pk_fail(PK_EINVAL, "pk_cost: negative size%s");
     if (E == 0) return PK_OK;
-    if (n_max > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_cost: more than 1024 trees per instance%s");
+    if (spec && spec->symmetry != 0 && spec->symmetry != 1 && spec->symmetry != 2 && spec->symmetry != 4)
+        return pk_fail(PK_EINVAL, "pk_cost: symmetry must be 0, 1, 2 or 4%s");
+    if (n_max > PK_MAX_TREES || (spec && (long long)n_max * pk_symmetry(*spec) > PK_MAX_TREES))
+        return pk_fail(PK_ERANGE, "pk_cost: more than 1024 (phenotype) trees per instance%s");
     if (!cost || (!xyt && n_max > 0)) return pk_fail(PK_EINVAL, "pk_cost: xyt and cost are required%s");
     if (spec->w_boundary != 0.f && !h) return pk_fail(PK_EINVAL, "pk_cost: boundary term needs h%s");
     if (spec->w_area != 0.f && !h) return pk_fail(PK_EINVAL, "pk_cost: area term needs h%s");
@@ -866,10 +910,10 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
         if (!L.vals || L.nx < 2 || L.ny < 2 || L.nt < 2)
             return pk_fail(PK_EINVAL, "pk_cost: LUT needs vals and at least 2 points per axis%s");
     }
-    const int T = pk_cost_threads(n_max);
+    const int T = pk_cost_threads(n_max * pk_symmetry(*spec));
     int cap_near, cap_items;
     pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
-    const size_t smem = pk_cost_smem_bytes(n_max, cap_near, cap_items);
+    const size_t smem = pk_cost_smem_bytes(n_max * pk_symmetry(*spec), cap_near, cap_items);
     cudaError_t err = cudaSuccess;
     switch (spec->pair_mode) {
 #define PK_CASE(M)                                                                                  \

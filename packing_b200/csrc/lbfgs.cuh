@@ -524,9 +524,10 @@ __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const
     const int N = 3 * n + 3;
     const int NM = 3 * n_max + 3;
     const int m = prm.history;
-    PkCostSmem sm = pk_cost_carve(smem, n_max, cap_near, cap_items);
+    const int nps = n_max * pk_symmetry(spec);   // phenotype trees sized in shared memory
+    PkCostSmem sm = pk_cost_carve(smem, nps, cap_near, cap_items);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
-    float* x = (float*)(smem + pk_cost_smem_bytes(n_max, cap_near, cap_items));
+    float* x = (float*)(smem + pk_cost_smem_bytes(nps, cap_near, cap_items));
     float* g = x + NM;
     float* pg = g + NM;
     float* d = pg + NM;
@@ -604,13 +605,14 @@ __global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict
     const int N = 3 * n + 3;
     const int NM = 3 * n_max + 3;
     const int m = prm.history;
+    const int nps = n_max * pk_symmetry(spec);
     PkRelaxParams p = prm;
     p.max_iter = J->max_iter;
     p.max_eval = J->max_iter * 5 / 4;
     p.final_eval = 1;
-    PkCostSmem sm = pk_cost_carve(pk_smem, n_max, cap_near, cap_items);
+    PkCostSmem sm = pk_cost_carve(pk_smem, nps, cap_near, cap_items);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
-    float* x = (float*)(pk_smem + pk_cost_smem_bytes(n_max, cap_near, cap_items));
+    float* x = (float*)(pk_smem + pk_cost_smem_bytes(nps, cap_near, cap_items));
     float* g = x + NM;
     float* pg = g + NM;
     float* d = pg + NM;
@@ -649,10 +651,13 @@ __global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict
     }
 }
 
-static size_t pk_relax_smem_bytes(int n_max, int cap_near, int cap_items, int m)
+// n_max genotype trees (the L-BFGS vectors), sym images of each (the cost's
+// per-tree arrays).
+static size_t pk_relax_smem_bytes(int n_max, int sym, int cap_near, int cap_items, int m)
 {
     const int NM = 3 * n_max + 3;
-    return pk_cost_smem_bytes(n_max, cap_near, cap_items) + ((size_t)4 * NM + 2 * (size_t)m + pk_canon_red_len(NM)) * 4;
+    return pk_cost_smem_bytes(n_max * sym, cap_near, cap_items) +
+           ((size_t)4 * NM + 2 * (size_t)m + pk_canon_red_len(NM)) * 4;
 }
 
 // Threads per CTA of the relaxation kernels: the caller's choice (an
@@ -758,11 +763,15 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
         return pk_fail(PK_EINVAL, "pk_relax: boundary / area terms need h%s");
     if (spec->pair_mode == PK_PAIR_LUT && !spec->lut.vals) return pk_fail(PK_EINVAL, "pk_relax: LUT without vals%s");
     int T = 0;
-    rc = pk_relax_threads(n_max, prm->threads, &T, "pk_relax");
+    if (spec->symmetry != 0 && spec->symmetry != 1 && spec->symmetry != 2 && spec->symmetry != 4)
+        return pk_fail(PK_EINVAL, "pk_relax: symmetry must be 0, 1, 2 or 4%s");
+    const int sym = pk_symmetry(*spec);
+    if ((long long)n_max * sym > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_relax: more than 1024 phenotype trees%s");
+    rc = pk_relax_threads(n_max * sym, prm->threads, &T, "pk_relax");
     if (rc) return rc;
     int cap_near, cap_items;
     pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
-    const size_t smem = pk_relax_smem_bytes(n_max, cap_near, cap_items, prm->history);
+    const size_t smem = pk_relax_smem_bytes(n_max, sym, cap_near, cap_items, prm->history);
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaSuccess;
     int grid = E;
@@ -808,11 +817,15 @@ extern "C" int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* poo
     if (!jobs || !list || !pool) return pk_fail(PK_EINVAL, "pk_relax_jobs: NULL pointer%s");
     if (spec->pair_mode == PK_PAIR_LUT && !spec->lut.vals) return pk_fail(PK_EINVAL, "pk_relax_jobs: LUT without vals%s");
     int T = 0;
-    rc = pk_relax_threads(n_max, prm->threads, &T, "pk_relax_jobs");
+    if (spec->symmetry != 0 && spec->symmetry != 1 && spec->symmetry != 2 && spec->symmetry != 4)
+        return pk_fail(PK_EINVAL, "pk_relax_jobs: symmetry must be 0, 1, 2 or 4%s");
+    const int sym = pk_symmetry(*spec);
+    if ((long long)n_max * sym > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_relax_jobs: more than 1024 phenotype trees%s");
+    rc = pk_relax_threads(n_max * sym, prm->threads, &T, "pk_relax_jobs");
     if (rc) return rc;
     int cap_near, cap_items;
     pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
-    const size_t smem = pk_relax_smem_bytes(n_max, cap_near, cap_items, prm->history);
+    const size_t smem = pk_relax_smem_bytes(n_max, sym, cap_near, cap_items, prm->history);
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaSuccess;
     switch (spec->pair_mode) {

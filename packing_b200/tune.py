@@ -84,7 +84,8 @@ class RelaxTuner:
         return f"{p.name}|sm{p.major}{p.minor}|{p.multi_processor_count}sm"
 
     def key(self, n_max: int, spec: CostSpec, history: int) -> str:
-        return f"{self.gpu_name()}|n{bucket(n_max)}|{spec.pair}|m{int(history)}"
+        sym = int(getattr(spec, "symmetry", 1) or 1)
+        return f"{self.gpu_name()}|n{bucket(n_max)}|{spec.pair}|s{sym}|m{int(history)}"
 
     def _load(self):
         if self.cache_path and os.path.exists(self.cache_path):
@@ -108,8 +109,8 @@ class RelaxTuner:
         except OSError:
             pass
 
-    def candidates(self, n_max: int):
-        return [(t, p) for t in feasible_threads(n_max) for p in (False, True)]
+    def candidates(self, n_max: int, symmetry: int = 1):
+        return [(t, p) for t in feasible_threads(n_max * symmetry) for p in (False, True)]
 
     def measure(self, n_max: int, spec: CostSpec, history: int, E: int | None = None) -> dict:
         """Milliseconds per launch of every feasible shape on a sample batch
@@ -127,7 +128,7 @@ class RelaxTuner:
         work = torch.empty(max(1, workspace_floats([n_max] * E, history)), device=dev)
         st = torch.cuda.current_stream(dev)
         out = {}
-        for t, p in self.candidates(n_max):
+        for t, p in self.candidates(n_max, int(getattr(spec, "symmetry", 1) or 1)):
             prm = RelaxParams(n_iterations=self.iterations, history_size=history, max_step=0.01, final_eval=False,
                               threads=t, persistent=p)
             relax_into(xyt, h, xo, ho, loss, work, spec, prm)   # warm-up
@@ -150,6 +151,8 @@ class RelaxTuner:
             hit = self.table.get(k)
         if hit is None:
             nb = bucket(n_max)
+            if nb * int(getattr(spec, "symmetry", 1) or 1) > 1024:   # the kernel's phenotype limit
+                nb = n_max
             times = self.measure(nb, spec, history)
             (t, p), ms = min(times.items(), key=lambda kv: kv[1])
             hit = {"threads": int(t), "persistent": bool(p), "ms": ms, "n_tuned": nb,
@@ -161,7 +164,7 @@ class RelaxTuner:
 
     def tuned(self, params: RelaxParams, n_max: int, spec: CostSpec) -> RelaxParams:
         t, p = self.best(n_max, spec, params.history_size)
-        if 8 * t < n_max - 1:   # the bucket's choice is feasible for its upper edge, so for n_max too
+        if 8 * t < n_max * int(getattr(spec, "symmetry", 1) or 1) - 1:   # feasible at the bucket's edge, so here
             t = 0
         return dataclasses.replace(params, threads=t, persistent=p)
 

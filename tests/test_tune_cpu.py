@@ -35,7 +35,7 @@ def test_cache_round_trip(tmp_path, monkeypatch):
     from packing_b200.cost import CostSpec
     assert tn.best(100, CostSpec(), 10) == (128, True)
     data = json.loads(path.read_text())
-    assert data["TESTGPU|n128|area|m10"]["threads"] == 128
+    assert data["TESTGPU|n128|area|s1|m10"]["threads"] == 128
     tn2 = tune.RelaxTuner(0, cache_path=str(path))
     monkeypatch.setattr(tn2, "gpu_name", lambda: "TESTGPU")
     monkeypatch.setattr(tn2, "measure", lambda *a: pytest.fail("re-measured"))
