@@ -619,13 +619,15 @@ struct PkEvalOut {
 // Evaluate one instance.  X: 3n floats (global or shared), H: 3 floats or
 // NULL.  G: 3n floats or NULL (written, not accumulated); GH: 3 floats or
 // NULL.  Must be called by every thread of the block.
-template <int MODE>
+// SYM: the packing may be symmetric (spec.symmetry > 1); the plain
+// instantiation keeps no symmetry state in registers.
+template <int MODE, bool SYM>
 __device__ double pk_eval_instance(const float* X, int ng, const float* H, const PkCostSpec& spec,
                                    float* G, float* GH, const PkCostSmem& sm)
 {
     // ng genotype trees in X (3 ng floats); the cost is that of the n
     // phenotype trees, and G receives the genotype gradient
-    const int sym = pk_symmetry(spec);
+    const int sym = SYM ? pk_symmetry(spec) : 1;
     const int n = sym * ng;
     const int T = blockDim.x;
     const bool do_bnd = spec.w_boundary != 0.f && H != nullptr;
@@ -855,7 +857,7 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
     return total;
 }
 
-template <int MODE>
+template <int MODE, bool SYM>
 __global__ void __launch_bounds__(256, 3) pk_cost_kernel(const float* __restrict__ xyt, const int* __restrict__ offsets, int E,
                                int n_max, const float* __restrict__ h, PkCostSpec spec,
                                float* __restrict__ cost, float* __restrict__ grad,
@@ -870,10 +872,10 @@ __global__ void __launch_bounds__(256, 3) pk_cost_kernel(const float* __restrict
         if (threadIdx.x == 0) cost[e] = __int_as_float(0x7fc00000);   // NaN marks a bad offset
         return;
     }
-    PkCostSmem sm = pk_cost_carve(pk_smem, n_max * pk_symmetry(spec), cap_near, cap_items);
+    PkCostSmem sm = pk_cost_carve(pk_smem, n_max * (SYM ? pk_symmetry(spec) : 1), cap_near, cap_items);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
     __syncthreads();
-    const double tot = pk_eval_instance<MODE>(xyt + (size_t)base * 3, n, h ? h + 3 * e : nullptr, spec,
+    const double tot = pk_eval_instance<MODE, SYM>(xyt + (size_t)base * 3, n, h ? h + 3 * e : nullptr, spec,
                                               grad ? grad + (size_t)base * 3 : nullptr,
                                               grad_h ? grad_h + 3 * e : nullptr, sm);
     if (threadIdx.x == 0) cost[e] = (float)tot;
@@ -918,13 +920,21 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
     switch (spec->pair_mode) {
 #define PK_CASE(M)                                                                                  \
     case M:                                                                                         \
-        err = cudaFuncSetAttribute(pk_cost_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                   (int)smem);                                                      \
-        if (err == cudaSuccess) {                                                                   \
-            pk_cost_kernel<M><<<E, T, smem, st>>>(xyt, offsets, E, n_max, h, *spec, cost, grad,     \
-                                                  grad_h, cap_near, cap_items);                     \
-            err = cudaGetLastError();                                                               \
+        if (spec->symmetry > 1) {                                                                   \
+            err = cudaFuncSetAttribute(pk_cost_kernel<M, true>,                                     \
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+            if (err == cudaSuccess)                                                                 \
+                pk_cost_kernel<M, true><<<E, T, smem, st>>>(xyt, offsets, E, n_max, h, *spec, cost, \
+                                                            grad, grad_h, cap_near, cap_items);     \
+        } else {                                                                                    \
+            err = cudaFuncSetAttribute(pk_cost_kernel<M, false>,                                    \
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+            if (err == cudaSuccess)                                                                 \
+                pk_cost_kernel<M, false><<<E, T, smem, st>>>(xyt, offsets, E, n_max, h, *spec,      \
+                                                             cost, grad, grad_h, cap_near,          \
+                                                             cap_items);                            \
         }                                                                                           \
+        if (err == cudaSuccess) err = cudaGetLastError();                                           \
         break;
         PK_CASE(PK_PAIR_NONE)
         PK_CASE(PK_PAIR_AREA)

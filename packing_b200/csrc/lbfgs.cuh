@@ -404,7 +404,7 @@ struct PkRelaxVars {
 // history and v complete, so a later call with resume = true continues
 // exactly where this one stopped.  resume = false starts from x (evaluates
 // it first).  All threads of the block call it.
-template <int MODE>
+template <int MODE, bool SYM>
 __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float* al, float* ro, float* red, int& flip,
                                  float* S, float* Y, int n, bool use_h, const PkCostSpec& spec,
                                  const PkRelaxParams& prm, const PkCostSmem& sm, PkRelaxVars& v, bool resume,
@@ -416,7 +416,7 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
     for (;;) {
         if (need_eval) {
             __syncthreads();   // x complete
-            const double L = pk_eval_instance<MODE>(x, n, use_h ? x + 3 * n : nullptr, spec, want_grad ? g : nullptr,
+            const double L = pk_eval_instance<MODE, SYM>(x, n, use_h ? x + 3 * n : nullptr, spec, want_grad ? g : nullptr,
                                                     (want_grad && use_h) ? g + 3 * n : nullptr, sm);
             v.loss = (float)L;
         }
@@ -507,7 +507,7 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
 }
 
 // Relaxes instance e (all threads of the block call it; e is uniform).
-template <int MODE>
+template <int MODE, bool SYM>
 __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const float* __restrict__ h_in,
                                   const int* __restrict__ offsets, int E, int n_max, const PkCostSpec& spec,
                                   const PkRelaxParams& prm, float* __restrict__ xyt_out, float* __restrict__ h_out,
@@ -524,7 +524,7 @@ __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const
     const int N = 3 * n + 3;
     const int NM = 3 * n_max + 3;
     const int m = prm.history;
-    const int nps = n_max * pk_symmetry(spec);   // phenotype trees sized in shared memory
+    const int nps = n_max * (SYM ? pk_symmetry(spec) : 1);   // phenotype trees sized in shared memory
     PkCostSmem sm = pk_cost_carve(smem, nps, cap_near, cap_items);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
     float* x = (float*)(smem + pk_cost_smem_bytes(nps, cap_near, cap_items));
@@ -545,7 +545,7 @@ __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const
     v.it = 0; v.evals = 1; v.hlen = 0; v.hstart = 0; v.active = 1;
     v.H = 1.f; v.loss = 0.f; v.loss0 = 0.f; v.ploss = 0.f; v.t = 0.f;
     unsigned long long hist_streamed = 0;
-    pk_relax_iterate<MODE>(x, g, pg, d, al, ro, red, flip, S, Y, n, h_in != nullptr, spec, prm, sm, v, false,
+    pk_relax_iterate<MODE, SYM>(x, g, pg, d, al, ro, red, flip, S, Y, n, h_in != nullptr, spec, prm, sm, v, false,
                            prm.max_iter, hist_streamed);
     __syncthreads();
     for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) xyt_out[(size_t)base * 3 + k] = x[k];
@@ -564,7 +564,7 @@ __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const
 // One CTA per instance, or (persistent) one CTA per resident slot walking the
 // launch order with a stride of the grid: CTA b relaxes order[b],
 // order[b + G], ...; largest-first orders keep the CTAs' loads even.
-template <int MODE, bool PERSISTENT>
+template <int MODE, bool PERSISTENT, bool SYM>
 __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in,
                                 const int* __restrict__ offsets, const int* __restrict__ order, int E, int n_max,
                                 PkCostSpec spec, PkRelaxParams prm, float* __restrict__ xyt_out,
@@ -573,11 +573,11 @@ __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restric
 {
     extern __shared__ __align__(16) unsigned char pk_smem[];
     if (!PERSISTENT) {
-        pk_relax_instance<MODE>(order ? order[blockIdx.x] : blockIdx.x, xyt_in, h_in, offsets, E, n_max, spec, prm,
+        pk_relax_instance<MODE, SYM>(order ? order[blockIdx.x] : blockIdx.x, xyt_in, h_in, offsets, E, n_max, spec, prm,
                                 xyt_out, h_out, loss_out, iters_out, work, cap_near, cap_items, pk_smem);
     } else {
         for (int k = blockIdx.x; k < E; k += gridDim.x) {
-            pk_relax_instance<MODE>(order ? order[k] : k, xyt_in, h_in, offsets, E, n_max, spec, prm, xyt_out, h_out,
+            pk_relax_instance<MODE, SYM>(order ? order[k] : k, xyt_in, h_in, offsets, E, n_max, spec, prm, xyt_out, h_out,
                                     loss_out, iters_out, work, cap_near, cap_items, pk_smem);
             __syncthreads();   // shared state is reused by the next instance
         }
@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restric
 // whatever other jobs share its launches and however its iterations are
 // split into chunks.
 // ---------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, bool SYM>
 __global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict__ jobs, const int* __restrict__ list,
                                      int njobs, float* __restrict__ pool, int n_max, PkCostSpec spec,
                                      PkRelaxParams prm, int chunk_iters, int cap_near, int cap_items)
@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict
     const int N = 3 * n + 3;
     const int NM = 3 * n_max + 3;
     const int m = prm.history;
-    const int nps = n_max * pk_symmetry(spec);
+    const int nps = n_max * (SYM ? pk_symmetry(spec) : 1);
     PkRelaxParams p = prm;
     p.max_iter = J->max_iter;
     p.max_eval = J->max_iter * 5 / 4;
@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict
     if (!resume) { v.it = 0; v.evals = 1; v.hlen = 0; v.hstart = 0; v.H = 1.f; }
     unsigned long long hs = 0;
     const int it_stop = min(p.max_iter, v.it + max(chunk_iters, 1));
-    const bool finished = pk_relax_iterate<MODE>(x, g, pg, d, al, ro, red, flip, S, Y, n, true, spec, p, sm, v,
+    const bool finished = pk_relax_iterate<MODE, SYM>(x, g, pg, d, al, ro, red, flip, S, Y, n, true, spec, p, sm, v,
                                                  resume, it_stop, hs);
     __syncthreads();
     for (int k = threadIdx.x; k < N; k += blockDim.x) {
@@ -689,12 +689,12 @@ static int pk_relax_threads(int n_max, int want, int* T, const char* who)
 // attribute call (they can then be captured into a CUDA graph).
 static cudaError_t pk_set_smem(const void* fn, int slot, size_t smem)
 {
-    static size_t done[64][16];
+    static size_t done[64][32];
     static std::mutex mu;
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
-    if (dev < 0 || dev >= 64 || slot < 0 || slot >= 16) return cudaErrorInvalidValue;
+    if (dev < 0 || dev >= 64 || slot < 0 || slot >= 32) return cudaErrorInvalidValue;
     std::lock_guard<std::mutex> lock(mu);
     if (smem <= done[dev][slot]) return cudaSuccess;
     err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -776,21 +776,22 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
     cudaError_t err = cudaSuccess;
     int grid = E;
     switch (spec->pair_mode) {
+#define PK_R3(M, P, S)                                                                                   \
+    {                                                                                                    \
+        err = pk_set_smem((const void*)pk_relax_kernel<M, P, S>, 4 + M + 4 * (P) + 8 * (S), smem);      \
+        if (err == cudaSuccess && (P))                                                                   \
+            err = pk_resident_grid((const void*)pk_relax_kernel<M, P, S>, T, smem, E, &grid);            \
+        if (err == cudaSuccess)                                                                          \
+            pk_relax_kernel<M, P, S><<<grid, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, \
+                                                            xyt_out, h_out, loss_out, iters_out, work, cap_near, \
+                                                            cap_items);                                  \
+    }
 #define PK_R(M)                                                                                          \
     case M:                                                                                              \
         if (prm->persistent) {                                                                           \
-            err = pk_set_smem((const void*)pk_relax_kernel<M, true>, 12 + M, smem);                      \
-            if (err == cudaSuccess) err = pk_resident_grid((const void*)pk_relax_kernel<M, true>, T, smem, E, &grid); \
-            if (err == cudaSuccess)                                                                      \
-                pk_relax_kernel<M, true><<<grid, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, \
-                                                                xyt_out, h_out, loss_out, iters_out, work, cap_near, \
-                                                                cap_items);                              \
+            if (sym > 1) PK_R3(M, true, true) else PK_R3(M, true, false)                                 \
         } else {                                                                                         \
-            err = pk_set_smem((const void*)pk_relax_kernel<M, false>, 4 + M, smem);                      \
-            if (err == cudaSuccess)                                                                      \
-                pk_relax_kernel<M, false><<<grid, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, \
-                                                                 xyt_out, h_out, loss_out, iters_out, work, cap_near, \
-                                                                 cap_items);                             \
+            if (sym > 1) PK_R3(M, false, true) else PK_R3(M, false, false)                               \
         }                                                                                                \
         break;
         PK_R(PK_PAIR_NONE)
@@ -798,6 +799,7 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
         PK_R(PK_PAIR_SEP)
         PK_R(PK_PAIR_LUT)
 #undef PK_R
+#undef PK_R3
         default: return pk_fail(PK_EINVAL, "pk_relax: unknown pair_mode%s");
     }
     if (err != cudaSuccess) return pk_cuda_check(err, "pk_relax attribute");
@@ -831,9 +833,16 @@ extern "C" int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* poo
     switch (spec->pair_mode) {
 #define PK_J(M)                                                                                          \
     case M:                                                                                              \
-        err = pk_set_smem((const void*)pk_relax_jobs_kernel<M>, 8 + M, smem);                            \
+        if (sym > 1) {                                                                                   \
+            err = pk_set_smem((const void*)pk_relax_jobs_kernel<M, true>, 24 + M, smem);                  \
+            if (err == cudaSuccess)                                                                      \
+                pk_relax_jobs_kernel<M, true><<<njobs, T, smem, st>>>(jobs, list, njobs, pool, n_max, *spec, \
+                                                                      *prm, chunk_iters, cap_near, cap_items); \
+            break;                                                                                       \
+        }                                                                                                \
+        err = pk_set_smem((const void*)pk_relax_jobs_kernel<M, false>, 20 + M, smem);                     \
         if (err == cudaSuccess)                                                                          \
-            pk_relax_jobs_kernel<M><<<njobs, T, smem, st>>>(jobs, list, njobs, pool, n_max, *spec, *prm, chunk_iters, \
+            pk_relax_jobs_kernel<M, false><<<njobs, T, smem, st>>>(jobs, list, njobs, pool, n_max, *spec, *prm, chunk_iters, \
                                                             cap_near, cap_items);                        \
         break;
         PK_J(PK_PAIR_NONE)
