@@ -429,8 +429,11 @@ def measure_serve(args, dev):
 
 
 def measure_ragged_lut(args, dev):
-    """8192 instances, n log-uniform in [5, 200], LUT 256 x 256 x 360 built
-    from the overlap-area kernel; one launch relaxes them all."""
+    """8192 instances, n log-uniform in [5, 200], relaxed in one launch on the
+    GA's production fitness cost (pack_ga3.py:1475-1477): boundary + the
+    exact-separation LUT (max(0, v)^2) on the reference's default 900^3 grid
+    (pack_cost.py:1144-1215), built on the GPU and trimmed; the area term is
+    inactive at fixed h."""
     import torch
 
     from packing_b200 import pack_cuda_lut
@@ -439,10 +442,7 @@ def measure_ragged_lut(args, dev):
     from packing_b200.relax import RelaxParams, relax_into, workspace_floats
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    X = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 510, dtype=np.float32)[254:]
-    Y = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 256, dtype=np.float32)
-    T = np.linspace(-np.pi, np.pi, 360, dtype=np.float32)
-    lut = LookupTable.build_from_kernel("area", X=X, Y=Y, theta=T, trim_zeros=False, device=dev)
+    lut = LookupTable.build_exact_separation(device=dev)
     torch.cuda.synchronize(dev)
     build_s = time.perf_counter() - t0
     rng = np.random.default_rng(5)
@@ -454,7 +454,7 @@ def measure_ragged_lut(args, dev):
     off = torch.tensor(np.concatenate([[0], np.cumsum(sizes)]), dtype=torch.int32, device=dev)
     order = torch.tensor(np.argsort(-sizes, kind="stable"), dtype=torch.int32, device=dev)
     h = torch.from_numpy(hs).to(dev)
-    spec = CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=0.0, fixed_h=True, lut=lut)
+    spec = CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True, lut=lut)
     prm = RelaxParams(n_iterations=args.iters, history_size=args.history, max_step=0.01, final_eval=False)
     xo = torch.empty_like(flat)
     ho = torch.empty_like(h)
@@ -494,7 +494,7 @@ def measure_ragged_lut(args, dev):
             "launches": 1, "iterations": args.iters,
             "lut_cost_kernel_ms": lut_ms,
             "lut_kernel_algorithmic_GBps": near_total * 32 / (lut_ms * 1e-3) / 1e9,
-            "note": "one ragged launch (largest first); LUT tabulates the overlap area"}
+            "note": "one ragged launch (largest first); production exact-separation LUT, 900^3 grid trimmed"}
 
 
 def measure_ga_step(args, dev):

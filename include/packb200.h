@@ -144,6 +144,19 @@ int pk_overlap_lut(const float* xyt, const int* offsets, int E, int n_uniform, c
 int pk_lut_build(const float* X, int nx, const float* Y, int ny, const float* T, int nt, int pair_mode,
                  float* vals, void* stream);
 
+/* Fills vals (nx, ny, nt) with the exact signed separation of a tree at the
+ * origin and one at (X[ix], Y[iy]) rotated by T[it]: + the distance to the
+ * boundary of their Minkowski difference (the union of the 16 convex piece
+ * differences) when the trees overlap, - that distance when they do not --
+ * pack_minkowski.separation_distance (pack_minkowski.py:210-266), the
+ * function CollisionCostExactSeparation tabulates through
+ * LookupTable.build_from_function (pack_cost.py:1144-1215), evaluated in FP64
+ * on the GPU.  Each slice uses the rotation angle the reference's float32
+ * theta gives through np.degrees and shapely's rotate.  X, Y, T are device
+ * float32 vectors; synchronises the stream. */
+int pk_lut_build_exact_sep(const float* X, int nx, const float* Y, int ny, const float* T, int nt,
+                           float* vals, void* stream);
+
 /* ---- batched linear assignment (lap_batch.py) ------------------------- */
 
 /* Hungarian on B float32 N x N matrices (solve_lap_batch with the default

@@ -98,6 +98,7 @@ SIGNATURES = {
     "pk_boundary": [_P, _P, _I, _I, _P, _P, _P, _P],
     "pk_overlap_lut": [_P, _P, _I, _I, ctypes.POINTER(PkLut), _P, _P, _P],
     "pk_lut_build": [_P, _I, _P, _I, _P, _I, _I, _P, _P],
+    "pk_lut_build_exact_sep": [_P, _I, _P, _I, _P, _I, _P, _P],
     "pk_lap_solve": [_P, _I, _I, _P, _P, _P, _P],
     "pk_diversity_matrix": [_P, _P, _I, _I, _I, _I, _P, _P],
     "pk_diversity_costs": [_P, _P, _I, _I, _I, _I, _P, _P],

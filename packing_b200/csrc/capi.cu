@@ -10,6 +10,7 @@
 #include "validate.cuh"
 #include "wolfe.cuh"
 #include "crystal.cuh"
+#include "minkowski.cuh"
 
 extern "C" int pk_version(void) { return 1; }
 

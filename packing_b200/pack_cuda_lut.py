@@ -14,7 +14,10 @@ launch per distinct tree count).
 analytic overlap-area (or separation) kernel, the same quantity
 ``CollisionCost._ensure_lut_initialized`` tabulates
 (``pack_cost.py:322-377``); ``build_from_function`` accepts any CPU
-``eval_fn`` exactly like the reference.
+``eval_fn`` exactly like the reference.  ``build_exact_separation`` builds
+the production table of ``CollisionCostExactSeparation``
+(``pack_cost.py:1144-1215``) -- the signed Minkowski separation the
+reference tabulates slice by slice with shapely -- on the GPU in FP64.
 """
 from __future__ import annotations
 
@@ -133,12 +136,37 @@ class LookupTable:
             vals = torch.from_numpy(np.ascontiguousarray(v)).to(dev)
         return cls(X=X, Y=Y, theta=theta, vals=vals, apply_quadratic_transform=apply_quadratic_transform)
 
-    @staticmethod
-    def _trim_zero_edges(X, Y, theta, vals, verbose=True):
-        """Drop all-non-positive edge slabs, keeping one non-positive row/column
-        at each X and Y edge (pack_cuda_lut.py:171-254)."""
-        N_x, N_y, N_t = vals.shape
+    @classmethod
+    def build_exact_separation(cls, X=None, Y=None, theta=None, N_x=900, N_y=900, N_theta=900, trim_zeros=True,
+                               device=None) -> "LookupTable":
+        """The table of ``CollisionCostExactSeparation`` (pack_cost.py:1144-1215):
+        the signed Minkowski separation of pack_minkowski.separation_distance
+        tabulated on the reference's default 900^3 grid, built on the GPU in
+        FP64 and stored as float32, with the per-pair ``max(0, v)^2``
+        transform on."""
+        dX, dY, dT = cls.default_grid(N_x, N_y, N_theta)
+        X = dX if X is None else np.asarray(X, np.float32)
+        Y = dY if Y is None else np.asarray(Y, np.float32)
+        theta = dT if theta is None else np.asarray(theta, np.float32)
+        dev = torch.device(device or "cuda")
+        _lib.ensure_init(dev)
+        Xd = torch.from_numpy(np.ascontiguousarray(X)).to(dev)
+        Yd = torch.from_numpy(np.ascontiguousarray(Y)).to(dev)
+        Td = torch.from_numpy(np.ascontiguousarray(theta)).to(dev)
+        vals = torch.empty((len(X), len(Y), len(theta)), device=dev, dtype=torch.float32)
+        with torch.cuda.device(dev):
+            rc = _lib.load().pk_lut_build_exact_sep(_lib.ptr(Xd), len(X), _lib.ptr(Yd), len(Y), _lib.ptr(Td),
+                                                    len(theta), _lib.ptr(vals),
+                                                    ctypes.c_void_p(_lib.stream_handle(None, dev)))
+        _lib.check(rc, "pk_lut_build_exact_sep")
+        if trim_zeros:
+            X, Y, theta, vals = cls._trim_zero_edges_device(X, Y, theta, vals)
+        return cls(X=X, Y=Y, theta=theta, vals=vals, apply_quadratic_transform=True)
 
+    @staticmethod
+    def _trim_ranges(mx_x, mx_y, mx_t):
+        """Index ranges kept by the trim: the positive span of each axis's
+        maxima, widened by one row/column on X and Y (pack_cuda_lut.py:171-254)."""
         def rng(mx, keep):
             pos = np.where(mx > 0)[0]
             if len(pos) == 0:
@@ -146,10 +174,24 @@ class LookupTable:
             if keep:
                 return max(0, pos[0] - 1), min(len(mx) - 1, pos[-1] + 1)
             return pos[0], pos[-1]
+        return rng(mx_x, True), rng(mx_y, True), rng(mx_t, False)
 
-        xs, xe = rng(np.max(vals, axis=(1, 2)), True)
-        ys, ye = rng(np.max(vals, axis=(0, 2)), True)
-        ts, te = rng(np.max(vals, axis=(0, 1)), False)
+    @classmethod
+    def _trim_zero_edges_device(cls, X, Y, theta, vals):
+        """``_trim_zero_edges`` on a device table, without copying it to the host."""
+        (xs, xe), (ys, ye), (ts, te) = cls._trim_ranges(vals.amax(dim=(1, 2)).cpu().numpy(),
+                                                        vals.amax(dim=(0, 2)).cpu().numpy(),
+                                                        vals.amax(dim=(0, 1)).cpu().numpy())
+        v = vals[xs:xe + 1, ys:ye + 1, ts:te + 1].contiguous()
+        return X[xs:xe + 1], Y[ys:ye + 1], theta[ts:te + 1], v
+
+    @classmethod
+    def _trim_zero_edges(cls, X, Y, theta, vals, verbose=True):
+        """Drop all-non-positive edge slabs, keeping one non-positive row/column
+        at each X and Y edge (pack_cuda_lut.py:171-254)."""
+        N_x, N_y, N_t = vals.shape
+        (xs, xe), (ys, ye), (ts, te) = cls._trim_ranges(np.max(vals, axis=(1, 2)), np.max(vals, axis=(0, 2)),
+                                                        np.max(vals, axis=(0, 1)))
         out = (X[xs:xe + 1], Y[ys:ye + 1], theta[ts:te + 1], vals[xs:xe + 1, ys:ye + 1, ts:te + 1])
         if verbose:
             print(f"Trimming non-positive edges: X {N_x}->{len(out[0])}, Y {N_y}->{len(out[1])}, "
