@@ -498,20 +498,26 @@ def measure_ragged_lut(args, dev):
 
 
 def measure_ga_step(args, dev):
-    """2048 packings of n = 100: Hungarian matching on 100 x 100 costs,
-    crossover + Gaussian mutation (0.05, 5 deg), 100-iteration relaxation."""
+    """2048 offspring of a population of n = 100 packings: the batched
+    Hungarian on 100 x 100 tree-assignment costs (the diversity measure's
+    solve), the GA's default move selector in one launch, and one full
+    offspring generation (clone, moves, 80-iteration relaxation on the GA's
+    fitness cost with the exact-separation LUT)."""
     import torch
 
     from packing_b200 import lap_batch
-    from packing_b200.ga_step import generation_step, matching_costs
+    from packing_b200 import pack_move as PM
+    from packing_b200.ga_step import default_moves, fitness_spec, generation_step, matching_costs
+    from packing_b200.pack_cuda_lut import LookupTable
     P, n = args.ga_P, 100
     xyt, h = workload(P, n, seed=21)
     pop = torch.from_numpy(xyt).to(dev)
     hh = torch.from_numpy(h).to(dev)
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(0)
-    partners = torch.randperm(P, generator=gen, device=dev)
-    C = matching_costs(pop, pop[partners])
+    tg = torch.Generator(device=dev)
+    tg.manual_seed(0)
+    parents = torch.randint(0, P, (P,), generator=tg, device=dev)
+    mates = (parents + torch.randint(1, P, (P,), generator=tg, device=dev)) % P   # never the parent itself
+    C = matching_costs(pop, pop[mates])
     lap_batch.solve_lap_batch(C)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -521,16 +527,37 @@ def measure_ga_step(args, dev):
     e1.record()
     torch.cuda.synchronize(dev)
     lap_ms = e0.elapsed_time(e1) / 3
-    generation_step(pop, partners, hh, gen, iterations=args.ga_iters)
+    # the move selector alone, on clones
+    moves = default_moves()
+    gen = PM.MoveGenerator(seed=5)
+    old = PM.Genotype(pop, hh)
+    child = PM.Genotype(pop.index_select(0, parents).contiguous(), hh.index_select(0, parents).contiguous())
+    rows = torch.arange(P, device=dev)
+    moves.do_move_vec(child, rows, old, mates, gen)
+    torch.cuda.synchronize(dev)
+    reps = 10
+    e0.record()
+    for _ in range(reps):
+        PM.apply_moves([(m[0], m[2]) for m in moves.moves], child, rows, old, mates, gen, check=False)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    moves_ms = e0.elapsed_time(e1) / reps
+    lut = LookupTable.build_exact_separation(device=dev)
+    spec = fitness_spec(lut)
+    generation_step(pop, hh, parents, mates, gen, spec, moves, iterations=args.ga_iters)
     torch.cuda.synchronize(dev)
     e0.record()
-    out, loss, rm = generation_step(pop, partners, hh, gen, iterations=args.ga_iters)
+    out, hout, loss, chosen = generation_step(pop, hh, parents, mates, gen, spec, moves, iterations=args.ga_iters)
     e1.record()
     torch.cuda.synchronize(dev)
     step_ms = e0.elapsed_time(e1)
+    counts = torch.bincount(chosen[chosen >= 0].long(), minlength=len(moves.moves)).cpu().tolist()
     return {"population": P, "n": n, "lap_instances_per_s": P / (lap_ms * 1e-3), "lap_ms": lap_ms,
-            "lap_hbm_GBps": P * n * n * 4 / (lap_ms * 1e-3) / 1e9, "generation_ms": step_ms,
-            "generations_per_s": 1e3 / step_ms, "relax_iterations": args.ga_iters}
+            "lap_hbm_GBps": P * n * n * 4 / (lap_ms * 1e-3) / 1e9,
+            "moves_ms": moves_ms, "moves_rows_per_s": P / (moves_ms * 1e-3),
+            "moves_chosen": dict(zip([m[1] for m in moves.moves], counts)),
+            "generation_ms": step_ms, "generations_per_s": 1e3 / step_ms, "relax_iterations": args.ga_iters,
+            "relax_cost": "GA fitness: boundary + exact-separation LUT (900^3, trimmed), fixed h"}
 
 
 def measure_legalize(args, dev):
@@ -651,7 +678,7 @@ def main():
     ap.add_argument("--serve-plain-batch", dest="serve_plain_batch", type=int, default=256)
     ap.add_argument("--lut-E", dest="lut_E", type=int, default=8192)
     ap.add_argument("--ga-P", dest="ga_P", type=int, default=2048)
-    ap.add_argument("--ga-iters", dest="ga_iters", type=int, default=100)
+    ap.add_argument("--ga-iters", dest="ga_iters", type=int, default=80)
     ap.add_argument("--legal-E", dest="legal_E", type=int, default=64)
     ap.add_argument("--quick", action="store_true", help="headline timing only")
     ap.add_argument("--no-tune", dest="no_tune", action="store_true",

@@ -336,6 +336,82 @@ int pk_relax_noalloc(const float* xyt_in, const float* h_in, int E, int n, const
  * (then h = (side, 0, 0)).  xyt_out may alias xyt_in. */
 int pk_snap(const float* xyt_in, const float* h_in, int E, int n, float* xyt_out, float* h_out, void* stream);
 
+/* ---- GA offspring moves (pack_move.py) -------------------------------- */
+
+#define PK_MOVE_RANDOM_TREE 0     /* MoveRandomTree,   pack_move.py:161 */
+#define PK_MOVE_JIGGLE_TREE 1     /* JiggleRandomTree, :191 */
+#define PK_MOVE_JIGGLE_CLUSTER 2  /* JiggleCluster,    :227 */
+#define PK_MOVE_TRANSLATE 3       /* Translate,        :301 */
+#define PK_MOVE_TWIST 4           /* Twist,            :336 */
+#define PK_MOVE_CROSSOVER 5       /* Crossover,        :406 */
+#define PK_MOVE_CROSSOVER2 6      /* Crossover2,       :635 */
+#define PK_MAX_MOVE_TYPES 16
+
+#define PK_GENO_SQUARE 0          /* SolutionCollectionSquare */
+#define PK_GENO_SYM90 1           /* SolutionCollectionSquareSymmetric90 */
+#define PK_GENO_SYM180 2          /* SolutionCollectionSquareSymmetric180 */
+
+#define PK_XDIST_STRIPE 0         /* Crossover2.distance_function */
+#define PK_XDIST_SQUARE 1
+#define PK_XDIST_SQUARE90 2
+#define PK_XDIST_SQUARE180 3
+
+/* One entry of a MoveSelector: the move class and its fields. */
+typedef struct PkMove {
+    int type;                          /* PK_MOVE_* */
+    int respect_edge_spacer_filter;
+    double max_xy_move, max_theta_move;        /* JiggleRandomTree, JiggleCluster */
+    int min_n_trees, max_n_trees;              /* JiggleCluster; min_n_trees also for the crossovers */
+    double max_n_trees_ratio;                  /* Crossover, Crossover2 */
+    double min_radius, max_radius;             /* Twist */
+    int simple_mate_location;                  /* Crossover */
+    int distance_function;                     /* Crossover2: PK_XDIST_* */
+    int decouple_mate_location;                /* Crossover2 */
+    int use_edge_clearance_when_decoupled;     /* Crossover2 */
+    int do_90_rotation;                        /* Crossover2 */
+} PkMove;
+
+/* The population's genotype class and its move-location filter
+ * (kaggle_support.py:454-535): EdgeSpacerDummy (spacer 0) or
+ * EdgeSpacerBasic (spacer 1). */
+typedef struct PkGenotype {
+    int kind;                 /* PK_GENO_* of the population: move centres, N_trees */
+    int mate_kind;            /* PK_GENO_* of the mate collection: canonicalisation, N_trees */
+    int filter;               /* filter_move_locations_with_edge_spacer */
+    int spacer;
+    double margin;            /* filter_move_locations_margin */
+    double dist_x, dist_y, dist_corner;
+} PkGenotype;
+
+/* MoveSelector (pack_move.py:119-158): cum_prob holds the float32 cumulative
+ * normalised weights; a draw u picks the first move with u <= cum_prob. */
+typedef struct PkMoveSet {
+    int n_moves;
+    double cum_prob[PK_MAX_MOVE_TYPES];
+    PkMove moves[PK_MAX_MOVE_TYPES];
+    PkGenotype geno;
+} PkMoveSet;
+
+/* Move.do_move_vec of a MoveSelector (pack_move.py:31-55, 119-158) on the
+ * rows inds_to_do (C,) of xyt (E, n, 3), in place, with mates
+ * mate_xyt[inds_mate] (mate_xyt (M, n, 3), mate_h (M, 3)); h (E, 3).  One CTA
+ * per row: the move is chosen and applied with random draws from
+ * Philox4x32-10 keyed by seed and counted by (call, row position, draw), so a
+ * call is reproducible and independent of the batch split.  chosen (C,)
+ * int32 receives the move index (-1: none), status (device int, nullable)
+ * is or-ed with 1 when a rejection sampler hit its limit, 2 for a request
+ * the reference rejects by assertion (edge-spacer filter on a 90-degree
+ * genotype, edge clearance above a quarter of the side) and 4 for a row or
+ * mate index out of range (that row is left unchanged).  Rows must be
+ * distinct and mate_xyt must not alias xyt; n <= 1024. */
+int pk_moves(float* xyt, const float* h, int E, int n, const int* inds_to_do, int C, const float* mate_xyt,
+             const float* mate_h, int M, const int* inds_mate, const PkMoveSet* set, uint64_t seed, uint64_t call,
+             int* chosen, int* status, void* stream);
+
+/* Philox4x32-10 draws of the move kernels (tests): out (count,) float64
+ * uniforms of (seed, call, row position), draws first .. first+count-1. */
+int pk_move_draws(uint64_t seed, uint64_t call, int row, int first, int count, double* out, void* stream);
+
 /* Floats of work needed by pk_relax: sizes_host (E,) host int32 tree counts
  * for a ragged batch, or NULL and n_uniform for a uniform one. */
 size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, int history);

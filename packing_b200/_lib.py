@@ -84,6 +84,37 @@ class PkJob(ctypes.Structure):
 PK_JOB_NEW, PK_JOB_RUNNING, PK_JOB_DONE = 0, 1, 2
 
 
+PK_MAX_MOVE_TYPES = 16
+
+
+class PkMove(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int), ("respect_edge_spacer_filter", ctypes.c_int),
+        ("max_xy_move", ctypes.c_double), ("max_theta_move", ctypes.c_double),
+        ("min_n_trees", ctypes.c_int), ("max_n_trees", ctypes.c_int),
+        ("max_n_trees_ratio", ctypes.c_double),
+        ("min_radius", ctypes.c_double), ("max_radius", ctypes.c_double),
+        ("simple_mate_location", ctypes.c_int), ("distance_function", ctypes.c_int),
+        ("decouple_mate_location", ctypes.c_int), ("use_edge_clearance_when_decoupled", ctypes.c_int),
+        ("do_90_rotation", ctypes.c_int),
+    ]
+
+
+class PkGenotype(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int), ("mate_kind", ctypes.c_int), ("filter", ctypes.c_int), ("spacer", ctypes.c_int),
+        ("margin", ctypes.c_double), ("dist_x", ctypes.c_double), ("dist_y", ctypes.c_double),
+        ("dist_corner", ctypes.c_double),
+    ]
+
+
+class PkMoveSet(ctypes.Structure):
+    _fields_ = [
+        ("n_moves", ctypes.c_int), ("cum_prob", ctypes.c_double * PK_MAX_MOVE_TYPES),
+        ("moves", PkMove * PK_MAX_MOVE_TYPES), ("geno", PkGenotype),
+    ]
+
+
 # (name, argtypes) of every exported entry point; include/packb200.h is the
 # authoritative declaration.
 _P, _I, _F, _D = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double
@@ -99,6 +130,9 @@ SIGNATURES = {
     "pk_overlap_lut": [_P, _P, _I, _I, ctypes.POINTER(PkLut), _P, _P, _P],
     "pk_lut_build": [_P, _I, _P, _I, _P, _I, _I, _P, _P],
     "pk_lut_build_exact_sep": [_P, _I, _P, _I, _P, _I, _P, _P],
+    "pk_moves": [_P, _P, _I, _I, _P, _I, _P, _P, _I, _P, ctypes.POINTER(PkMoveSet), ctypes.c_uint64, ctypes.c_uint64,
+                 _P, _P, _P],
+    "pk_move_draws": [ctypes.c_uint64, ctypes.c_uint64, _I, _I, _I, _P, _P],
     "pk_lap_solve": [_P, _I, _I, _P, _P, _P, _P],
     "pk_diversity_matrix": [_P, _P, _I, _I, _I, _I, _P, _P],
     "pk_diversity_costs": [_P, _P, _I, _I, _I, _I, _P, _P],

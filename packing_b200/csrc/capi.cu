@@ -11,6 +11,7 @@
 #include "wolfe.cuh"
 #include "crystal.cuh"
 #include "minkowski.cuh"
+#include "moves.cuh"
 
 extern "C" int pk_version(void) { return 1; }
 
