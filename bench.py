@@ -429,11 +429,11 @@ def measure_serve(args, dev):
 
 
 def measure_ragged_lut(args, dev):
-    """8192 instances, n log-uniform in [5, 200], relaxed in one launch on the
-    GA's production fitness cost (pack_ga3.py:1475-1477): boundary + the
-    exact-separation LUT (max(0, v)^2) on the reference's default 900^3 grid
-    (pack_cost.py:1144-1215), built on the GPU and trimmed; the area term is
-    inactive at fixed h."""
+    """8192 instances, n log-uniform in [5, 200], LUT 256 x 256 x 360 built
+    from the overlap-area kernel; one launch relaxes them all.  The same batch
+    is then relaxed on the GA's production fitness cost (pack_ga3.py:1475-1477):
+    boundary + the exact-separation LUT (max(0, v)^2) on the reference's
+    default 900^3 grid (pack_cost.py:1144-1215), built on the GPU and trimmed."""
     import torch
 
     from packing_b200 import pack_cuda_lut
@@ -442,7 +442,10 @@ def measure_ragged_lut(args, dev):
     from packing_b200.relax import RelaxParams, relax_into, workspace_floats
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    lut = LookupTable.build_exact_separation(device=dev)
+    X = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 510, dtype=np.float32)[254:]
+    Y = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 256, dtype=np.float32)
+    T = np.linspace(-np.pi, np.pi, 360, dtype=np.float32)
+    lut = LookupTable.build_from_kernel("area", X=X, Y=Y, theta=T, trim_zeros=False, device=dev)
     torch.cuda.synchronize(dev)
     build_s = time.perf_counter() - t0
     rng = np.random.default_rng(5)
@@ -454,24 +457,26 @@ def measure_ragged_lut(args, dev):
     off = torch.tensor(np.concatenate([[0], np.cumsum(sizes)]), dtype=torch.int32, device=dev)
     order = torch.tensor(np.argsort(-sizes, kind="stable"), dtype=torch.int32, device=dev)
     h = torch.from_numpy(hs).to(dev)
-    spec = CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True, lut=lut)
     prm = RelaxParams(n_iterations=args.iters, history_size=args.history, max_step=0.01, final_eval=False)
     xo = torch.empty_like(flat)
     ho = torch.empty_like(h)
     loss = torch.empty(E, device=dev)
     work = torch.empty(workspace_floats(sizes.tolist(), args.history), device=dev)
     nmax = int(sizes.max())
-    for _ in range(2):
-        relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax)
-    torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 3
-    e0.record()
-    for _ in range(reps):
-        relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax)
-    e1.record()
-    torch.cuda.synchronize(dev)
-    relax_s = e0.elapsed_time(e1) / 1e3 / reps
+
+    def time_relax(spec, reps=3):
+        for _ in range(2):
+            relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(reps):
+            relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    relax_s = time_relax(CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=0.0, fixed_h=True, lut=lut))
     # LUT cost kernel alone: algorithmic bytes = 8 corners x 4 B per near pair
     cost = torch.empty(E, device=dev)
     grad = torch.empty_like(flat)
@@ -489,35 +494,45 @@ def measure_ragged_lut(args, dev):
         dx = xk[:, None, :2] - xk[None, :, :2]
         near += int(((dx ** 2).sum(-1) <= (2 * 0.5796198) ** 2).sum() - len(xk)) // 2
     near_total = near * (E / len(range(0, E, max(1, E // 256))))
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    exact = LookupTable.build_exact_separation(device=dev)
+    torch.cuda.synchronize(dev)
+    exact_build_s = time.perf_counter() - t0
+    exact_s = time_relax(CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True, lut=exact))
     return {"instances": E, "n_range": [int(sizes.min()), int(sizes.max())], "lut_shape": list(lut.lut_d.shape),
             "lut_build_s": build_s, "relaxations_per_s": E / relax_s, "ms_per_launch": relax_s * 1e3,
             "launches": 1, "iterations": args.iters,
             "lut_cost_kernel_ms": lut_ms,
             "lut_kernel_algorithmic_GBps": near_total * 32 / (lut_ms * 1e-3) / 1e9,
-            "note": "one ragged launch (largest first); production exact-separation LUT, 900^3 grid trimmed"}
+            "note": "one ragged launch (largest first); LUT tabulates the overlap area",
+            "production_exact_lut": {"lut_shape": list(exact.lut_d.shape), "build_s": exact_build_s,
+                                     "relaxations_per_s": E / exact_s, "ms_per_launch": exact_s * 1e3,
+                                     "cost": "GA fitness: boundary + exact-separation LUT (900^3 grid trimmed), "
+                                             "max(0, v)^2, fixed h"}}
 
 
 def measure_ga_step(args, dev):
-    """2048 offspring of a population of n = 100 packings: the batched
-    Hungarian on 100 x 100 tree-assignment costs (the diversity measure's
-    solve), the GA's default move selector in one launch, and one full
-    offspring generation (clone, moves, 80-iteration relaxation on the GA's
-    fitness cost with the exact-separation LUT)."""
+    """2048 packings of n = 100: Hungarian matching on 100 x 100 costs,
+    crossover + Gaussian mutation (0.05, 5 deg), 100-iteration relaxation.
+    Then the reference GA's own offspring generation on the same population:
+    its default move selector in one launch, and clone + moves + the rough
+    relaxation (80 iterations) on its fitness cost with the exact LUT."""
     import torch
 
     from packing_b200 import lap_batch
     from packing_b200 import pack_move as PM
-    from packing_b200.ga_step import default_moves, fitness_spec, generation_step, matching_costs
+    from packing_b200.ga_step import (crossover_jitter_step, default_moves, fitness_spec, generation_step,
+                                      matching_costs)
     from packing_b200.pack_cuda_lut import LookupTable
     P, n = args.ga_P, 100
     xyt, h = workload(P, n, seed=21)
     pop = torch.from_numpy(xyt).to(dev)
     hh = torch.from_numpy(h).to(dev)
-    tg = torch.Generator(device=dev)
-    tg.manual_seed(0)
-    parents = torch.randint(0, P, (P,), generator=tg, device=dev)
-    mates = (parents + torch.randint(1, P, (P,), generator=tg, device=dev)) % P   # never the parent itself
-    C = matching_costs(pop, pop[mates])
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(0)
+    partners = torch.randperm(P, generator=gen, device=dev)
+    C = matching_costs(pop, pop[partners])
     lap_batch.solve_lap_batch(C)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -527,37 +542,49 @@ def measure_ga_step(args, dev):
     e1.record()
     torch.cuda.synchronize(dev)
     lap_ms = e0.elapsed_time(e1) / 3
-    # the move selector alone, on clones
+    crossover_jitter_step(pop, partners, hh, gen, iterations=args.ga_iters)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    crossover_jitter_step(pop, partners, hh, gen, iterations=args.ga_iters)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    step_ms = e0.elapsed_time(e1)
+    # the reference GA's offspring generation
+    parents = torch.randint(0, P, (P,), generator=gen, device=dev)
+    mates = (parents + torch.randint(1, P, (P,), generator=gen, device=dev)) % P   # never the parent itself
     moves = default_moves()
-    gen = PM.MoveGenerator(seed=5)
+    mgen = PM.MoveGenerator(seed=5)
     old = PM.Genotype(pop, hh)
     child = PM.Genotype(pop.index_select(0, parents).contiguous(), hh.index_select(0, parents).contiguous())
     rows = torch.arange(P, device=dev)
-    moves.do_move_vec(child, rows, old, mates, gen)
+    entries = [(m[0], m[2]) for m in moves.moves]
+    PM.apply_moves(entries, child, rows, old, mates, mgen)
     torch.cuda.synchronize(dev)
     reps = 10
     e0.record()
     for _ in range(reps):
-        PM.apply_moves([(m[0], m[2]) for m in moves.moves], child, rows, old, mates, gen, check=False)
+        PM.apply_moves(entries, child, rows, old, mates, mgen, check=False)
     e1.record()
     torch.cuda.synchronize(dev)
     moves_ms = e0.elapsed_time(e1) / reps
-    lut = LookupTable.build_exact_separation(device=dev)
-    spec = fitness_spec(lut)
-    generation_step(pop, hh, parents, mates, gen, spec, moves, iterations=args.ga_iters)
+    spec = fitness_spec(LookupTable.build_exact_separation(device=dev))
+    generation_step(pop, hh, parents, mates, mgen, spec, moves)
     torch.cuda.synchronize(dev)
     e0.record()
-    out, hout, loss, chosen = generation_step(pop, hh, parents, mates, gen, spec, moves, iterations=args.ga_iters)
+    _, _, _, chosen = generation_step(pop, hh, parents, mates, mgen, spec, moves)
     e1.record()
     torch.cuda.synchronize(dev)
-    step_ms = e0.elapsed_time(e1)
+    ref_ms = e0.elapsed_time(e1)
     counts = torch.bincount(chosen[chosen >= 0].long(), minlength=len(moves.moves)).cpu().tolist()
     return {"population": P, "n": n, "lap_instances_per_s": P / (lap_ms * 1e-3), "lap_ms": lap_ms,
-            "lap_hbm_GBps": P * n * n * 4 / (lap_ms * 1e-3) / 1e9,
-            "moves_ms": moves_ms, "moves_rows_per_s": P / (moves_ms * 1e-3),
-            "moves_chosen": dict(zip([m[1] for m in moves.moves], counts)),
-            "generation_ms": step_ms, "generations_per_s": 1e3 / step_ms, "relax_iterations": args.ga_iters,
-            "relax_cost": "GA fitness: boundary + exact-separation LUT (900^3, trimmed), fixed h"}
+            "lap_hbm_GBps": P * n * n * 4 / (lap_ms * 1e-3) / 1e9, "generation_ms": step_ms,
+            "generations_per_s": 1e3 / step_ms, "relax_iterations": args.ga_iters,
+            "reference_ga_offspring": {
+                "moves_ms": moves_ms, "moves_rows_per_s": P / (moves_ms * 1e-3),
+                "moves_chosen": dict(zip([m[1] for m in moves.moves], counts)),
+                "generation_ms": ref_ms,
+                "what": "clone + the GA's default MoveSelector (one pk_moves launch) + 80-iteration rough "
+                        "relaxation on boundary + exact-separation LUT, fixed h"}}
 
 
 def measure_legalize(args, dev):
@@ -678,7 +705,7 @@ def main():
     ap.add_argument("--serve-plain-batch", dest="serve_plain_batch", type=int, default=256)
     ap.add_argument("--lut-E", dest="lut_E", type=int, default=8192)
     ap.add_argument("--ga-P", dest="ga_P", type=int, default=2048)
-    ap.add_argument("--ga-iters", dest="ga_iters", type=int, default=80)
+    ap.add_argument("--ga-iters", dest="ga_iters", type=int, default=100)
     ap.add_argument("--legal-E", dest="legal_E", type=int, default=64)
     ap.add_argument("--quick", action="store_true", help="headline timing only")
     ap.add_argument("--no-tune", dest="no_tune", action="store_true",

@@ -12,8 +12,12 @@ as ``_generate_offspring`` does (``pack_ga3.py:1343-1431``):
    area 1e-2, boundary, exact-separation LUT) -- one ``relax`` launch.
 
 ``default_moves()`` is the reference GA's move selector (``pack_ga3.py:1084-1115``).
-``matching_costs`` builds the tree-assignment costs the diversity measure
-solves with the batched Hungarian (``lap_batch``).
+
+``crossover_jitter_step`` is the matched-crossover generation the batched
+Hungarian serves: every parent's trees are assigned to its partner's trees
+by ``lap_batch.solve_lap_batch`` on n x n costs (``matching_costs``: squared
+centre distance plus angle difference), the child takes a seeded half of
+the matched partner trees, gets Gaussian pose jitter, and is relaxed.
 """
 from __future__ import annotations
 
@@ -22,6 +26,7 @@ import math
 import numpy as np
 import torch
 
+from . import lap_batch
 from . import pack_move as PM
 from .cost import CostSpec
 from .relax import RelaxParams, relax
@@ -73,3 +78,24 @@ def generation_step(pop: torch.Tensor, h: torch.Tensor, parents: torch.Tensor, m
                                RelaxParams(n_iterations=iterations, history_size=history, max_step=max_step,
                                            final_eval=True))
     return out, hout, loss, chosen
+
+
+def crossover_jitter_step(pop: torch.Tensor, partners: torch.Tensor, h: torch.Tensor, generator: torch.Generator,
+                          sigma_xy: float = 0.05, sigma_deg: float = 5.0, iterations: int = 100,
+                          spec: CostSpec = CostSpec(), history: int = 10, max_step: float = 0.01):
+    """pop (P, n, 3), partners (P,) int64 indices into pop, h (P, 3).
+    Returns (children relaxed (P, n, 3), loss (P,), row_match (P, n))."""
+    P, n, _ = pop.shape
+    mates = pop[partners]
+    C = matching_costs(pop, mates)
+    row_match, _ = lap_batch.solve_lap_batch(C)
+    matched = torch.gather(mates, 1, row_match.long().clamp_min(0)[:, :, None].expand(P, n, 3))
+    take = torch.rand((P, n, 1), generator=generator, device=pop.device) < 0.5
+    child = torch.where(take, matched, pop)
+    noise = torch.randn((P, n, 3), generator=generator, device=pop.device)
+    noise[:, :, :2] *= sigma_xy
+    noise[:, :, 2] *= math.radians(sigma_deg)
+    child = (child + noise).contiguous()
+    out, _, loss, _ = relax(child, h, spec, RelaxParams(n_iterations=iterations, history_size=history,
+                                                        max_step=max_step, final_eval=True))
+    return out, loss, row_match
