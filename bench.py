@@ -656,6 +656,74 @@ def run_cost_case(args, dev):
     return out
 
 
+def run_exact_lut_case(args, dev):
+    """The exact-separation table build (pk_lut_build_exact_sep) on the
+    reference's default grid of --lut-n points per axis, untrimmed: --warmup
+    then --steps builds.  Algorithmic bytes: the float32 table written once.
+    A profiling case, not a benchmark metric."""
+    import torch
+
+    from packing_b200.pack_cuda_lut import LookupTable
+    N = args.lut_n
+    X, Y, T = LookupTable.default_grid(N, N, N)
+    for _ in range(args.warmup):
+        lut = LookupTable.build_exact_separation(X=X, Y=Y, theta=T, trim_zeros=False, device=dev)
+        del lut
+    torch.cuda.synchronize(dev)
+    t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        lut = LookupTable.build_exact_separation(X=X, Y=Y, theta=T, trim_zeros=False, device=dev)
+        torch.cuda.synchronize(dev)
+        t.append(time.perf_counter() - t0)
+        del lut
+    ms = 1e3 * min(t)
+    bytes_out = 4.0 * len(X) * len(Y) * len(T)
+    return {"case": "exact_lut", "grid": [len(X), len(Y), len(T)], "ms_per_build": ms,
+            "points_per_s": len(X) * len(Y) * len(T) / (ms * 1e-3), "table_write_GBps": bytes_out / (ms * 1e-3) / 1e9}
+
+
+def run_moves_case(args, dev):
+    """The GA's default move selector (pk_moves) on --ga-P clones of n = --n
+    packings, mates from the parent population: --warmup then --steps
+    launches timed with CUDA events.  Algorithmic bytes per row: the row read
+    and written (24 n B) plus the mate read (12 n B) for crossover rows.  A
+    profiling case, not a benchmark metric."""
+    import torch
+
+    from packing_b200 import pack_move as PM
+    from packing_b200.ga_step import default_moves
+    P, n = args.ga_P, args.n
+    xyt, h = workload(P, n, seed=21)
+    pop = torch.from_numpy(xyt).to(dev)
+    hh = torch.from_numpy(h).to(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    parents = torch.randint(0, P, (P,), generator=g, device=dev)
+    mates = (parents + torch.randint(1, P, (P,), generator=g, device=dev)) % P
+    old = PM.Genotype(pop, hh)
+    child = PM.Genotype(pop.index_select(0, parents).contiguous(), hh.index_select(0, parents).contiguous())
+    rows = torch.arange(P, device=dev)
+    moves = default_moves()
+    entries = [(m[0], m[2]) for m in moves.moves]
+    mgen = PM.MoveGenerator(seed=5)
+    chosen = PM.apply_moves(entries, child, rows, old, mates, mgen)
+    for _ in range(args.warmup):
+        PM.apply_moves(entries, child, rows, old, mates, mgen, check=False)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        PM.apply_moves(entries, child, rows, old, mates, mgen, check=False)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    cross = int(((chosen == 7) | (chosen == 8)).sum())
+    algo = P * 24.0 * n + cross * 12.0 * n
+    return {"case": "moves", "rows": P, "n": n, "ms_per_launch": ms, "rows_per_s": P / (ms * 1e-3),
+            "algorithmic_GBps": algo / (ms * 1e-3) / 1e9}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -710,9 +778,12 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline timing only")
     ap.add_argument("--no-tune", dest="no_tune", action="store_true",
                     help="default launch shape instead of the autotuned one (profiling captures)")
-    ap.add_argument("--case", default="relax", choices=["relax", "cost"],
+    ap.add_argument("--case", default="relax", choices=["relax", "cost", "exact_lut", "moves"],
                     help="relax: the headline; cost: the compound cost kernel alone on E packings, at the "
-                         "initial poses and after --iters iterations of relaxation (profiling captures)")
+                         "initial poses and after --iters iterations of relaxation; exact_lut: the exact-separation "
+                         "table build on --lut-n points per axis; moves: the GA's move selector on --ga-P rows of "
+                         "--n trees (profiling captures)")
+    ap.add_argument("--lut-n", dest="lut_n", type=int, default=900)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -731,7 +802,8 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=dev)
-    out = run_cost_case(args, dev) if args.case == "cost" else run_ours(args, rank, world, dev)
+    cases = {"cost": run_cost_case, "exact_lut": run_exact_lut_case, "moves": run_moves_case}
+    out = cases[args.case](args, dev) if args.case in cases else run_ours(args, rank, world, dev)
     if rank == 0:
         print(json.dumps(out))
     if world > 1:
