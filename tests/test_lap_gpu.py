@@ -126,3 +126,24 @@ def test_diversity_shortcut(cuda):
                                               ca, sa, mir).cpu().numpy()
         OD = O.diversity_shortcut(pop, ref, ca, sa, mir)
         np.testing.assert_allclose(D, OD, rtol=1e-5, atol=1e-5)
+
+
+def test_matched_crossover_generation(cuda):
+    """The matched-crossover generation: each parent's trees are assigned to
+    its partner's by the batched Hungarian (a permutation, equal to the
+    float32 restatement's), then crossover, jitter and relaxation give
+    finite children."""
+    from packing_b200.ga_step import crossover_jitter_step, matching_costs
+    P, n = 16, 20
+    x = torch.from_numpy(poses(P, n, seed=9)).to(cuda)
+    h = torch.zeros((P, 3), device=cuda)
+    h[:, 0] = float(np.sqrt(n * 0.2456875) * 1.3)
+    partners = torch.roll(torch.arange(P, device=cuda), 1)
+    g = torch.Generator(device=cuda)
+    g.manual_seed(1)
+    out, loss, rm = crossover_jitter_step(x, partners, h, g, iterations=20)
+    rm = rm.cpu().numpy()
+    assert all(np.array_equal(np.sort(r), np.arange(n)) for r in rm)
+    orm, _ = O.hungarian(matching_costs(x, x[partners]).cpu().numpy())
+    assert np.array_equal(rm, orm)
+    assert torch.isfinite(out).all() and torch.isfinite(loss).all()
