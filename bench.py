@@ -439,7 +439,7 @@ def measure_ragged_lut(args, dev):
     from packing_b200 import pack_cuda_lut
     from packing_b200.cost import CostSpec
     from packing_b200.pack_cuda_lut import LookupTable
-    from packing_b200.relax import RelaxParams, relax_into, workspace_floats
+    from packing_b200.relax import RelaxParams, relax_into, size_classes, workspace_floats
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     X = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 510, dtype=np.float32)[254:]
@@ -455,7 +455,9 @@ def measure_ragged_lut(args, dev):
     hs = np.concatenate([workload(1, int(nn), seed=0)[1] for nn in sizes])
     flat = torch.from_numpy(np.concatenate(xs)).to(dev)
     off = torch.tensor(np.concatenate([[0], np.cumsum(sizes)]), dtype=torch.int32, device=dev)
-    order = torch.tensor(np.argsort(-sizes, kind="stable"), dtype=torch.int32, device=dev)
+    order_h = np.argsort(-sizes, kind="stable")
+    order = torch.tensor(order_h, dtype=torch.int32, device=dev)
+    classes = size_classes(sizes[order_h])
     h = torch.from_numpy(hs).to(dev)
     prm = RelaxParams(n_iterations=args.iters, history_size=args.history, max_step=0.01, final_eval=False)
     xo = torch.empty_like(flat)
@@ -465,18 +467,20 @@ def measure_ragged_lut(args, dev):
     nmax = int(sizes.max())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def time_relax(spec, reps=3):
+    def time_relax(spec, cls=classes, reps=3):
         for _ in range(2):
-            relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax)
+            relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax, classes=cls)
         torch.cuda.synchronize(dev)
         e0.record()
         for _ in range(reps):
-            relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax)
+            relax_into(flat, h, xo, ho, loss, work, spec, prm, offsets=off, order=order, n_max=nmax, classes=cls)
         e1.record()
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) / 1e3 / reps
 
-    relax_s = time_relax(CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=0.0, fixed_h=True, lut=lut))
+    area_lut_spec = CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=0.0, fixed_h=True, lut=lut)
+    relax_s = time_relax(area_lut_spec)
+    single_s = time_relax(area_lut_spec, cls=None)
     # LUT cost kernel alone: algorithmic bytes = 8 corners x 4 B per near pair
     cost = torch.empty(E, device=dev)
     grad = torch.empty_like(flat)
@@ -501,13 +505,16 @@ def measure_ragged_lut(args, dev):
     exact_build_s = time.perf_counter() - t0
     exact_s = time_relax(CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True, lut=exact))
     return {"instances": E, "n_range": [int(sizes.min()), int(sizes.max())], "lut_shape": list(lut.lut_d.shape),
-            "lut_build_s": build_s, "relaxations_per_s": E / relax_s, "ms_per_launch": relax_s * 1e3,
-            "launches": 1, "iterations": args.iters,
+            "lut_build_s": build_s, "relaxations_per_s": E / relax_s, "ms_per_step": relax_s * 1e3,
+            "launches": len(classes), "iterations": args.iters,
+            "size_classes": [[c.n_max, c.count, c.threads] for c in classes],
+            "single_launch_relaxations_per_s": E / single_s,
             "lut_cost_kernel_ms": lut_ms,
             "lut_kernel_algorithmic_GBps": near_total * 32 / (lut_ms * 1e-3) / 1e9,
-            "note": "one ragged launch (largest first); LUT tabulates the overlap area",
+            "note": "largest first, one launch per size class (n_max, count, threads per CTA) side by side on "
+                    "forked streams; LUT tabulates the overlap area",
             "production_exact_lut": {"lut_shape": list(exact.lut_d.shape), "build_s": exact_build_s,
-                                     "relaxations_per_s": E / exact_s, "ms_per_launch": exact_s * 1e3,
+                                     "relaxations_per_s": E / exact_s, "ms_per_step": exact_s * 1e3,
                                      "cost": "GA fitness: boundary + exact-separation LUT (900^3 grid trimmed), "
                                              "max(0, v)^2, fixed h"}}
 
@@ -656,6 +663,48 @@ def run_cost_case(args, dev):
     return out
 
 
+def run_lut_case(args, dev):
+    """The LUT cost kernel alone (pk_overlap_lut, ragged) on the C4 batch:
+    --lut-E packings with n log-uniform in [5, 200], LUT 256 x 256 x 360 built
+    from the overlap-area kernel: --warmup then --steps launches.  Algorithmic
+    bytes: 8 corners x 4 B per near pair.  A profiling case, not a benchmark
+    metric."""
+    import torch
+
+    from packing_b200 import pack_cuda_lut
+    from packing_b200.pack_cuda_lut import LookupTable
+    X = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 510, dtype=np.float32)[254:]
+    Y = np.linspace(-2 * 0.5796198, 2 * 0.5796198, 256, dtype=np.float32)
+    T = np.linspace(-np.pi, np.pi, 360, dtype=np.float32)
+    lut = LookupTable.build_from_kernel("area", X=X, Y=Y, theta=T, trim_zeros=False, device=dev)
+    rng = np.random.default_rng(5)
+    E = args.lut_E
+    sizes = np.round(np.exp(rng.uniform(np.log(5), np.log(200), size=E))).astype(int)
+    xs = [workload(1, int(nn), seed=1000 + k)[0][0] for k, nn in enumerate(sizes)]
+    flat = torch.from_numpy(np.concatenate(xs)).to(dev)
+    off = torch.tensor(np.concatenate([[0], np.cumsum(sizes)]), dtype=torch.int32, device=dev)
+    nmax = int(sizes.max())
+    cost = torch.empty(E, device=dev)
+    grad = torch.empty_like(flat)
+    for _ in range(args.warmup):
+        pack_cuda_lut.overlap_multi_ensemble_ragged(flat, off, cost, lut, grad, n_max=nmax)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        pack_cuda_lut.overlap_multi_ensemble_ragged(flat, off, cost, lut, grad, n_max=nmax)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    near = 0
+    for x in xs:
+        d = x[:, None, :2] - x[None, :, :2]
+        near += int(((d ** 2).sum(-1) <= (2 * 0.5796198) ** 2).sum() - len(x)) // 2
+    return {"case": "lut", "instances": E, "lut_shape": list(lut.lut_d.shape), "ms_per_launch": ms,
+            "near_pairs": near, "lookups_per_s": near / (ms * 1e-3),
+            "algorithmic_GBps": near * 32 / (ms * 1e-3) / 1e9, "checksum": float(cost.double().sum())}
+
+
 def run_exact_lut_case(args, dev):
     """The exact-separation table build (pk_lut_build_exact_sep) on the
     reference's default grid of --lut-n points per axis, untrimmed: --warmup
@@ -778,10 +827,11 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline timing only")
     ap.add_argument("--no-tune", dest="no_tune", action="store_true",
                     help="default launch shape instead of the autotuned one (profiling captures)")
-    ap.add_argument("--case", default="relax", choices=["relax", "cost", "exact_lut", "moves"],
+    ap.add_argument("--case", default="relax", choices=["relax", "cost", "exact_lut", "moves", "lut"],
                     help="relax: the headline; cost: the compound cost kernel alone on E packings, at the "
                          "initial poses and after --iters iterations of relaxation; exact_lut: the exact-separation "
-                         "table build on --lut-n points per axis; moves: the GA's move selector on --ga-P rows of "
+                         "table build on --lut-n points per axis; lut: the LUT cost kernel alone on the C4 batch; "
+                         "moves: the GA's move selector on --ga-P rows of "
                          "--n trees (profiling captures)")
     ap.add_argument("--lut-n", dest="lut_n", type=int, default=900)
     args = ap.parse_args()
@@ -802,7 +852,7 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=dev)
-    cases = {"cost": run_cost_case, "exact_lut": run_exact_lut_case, "moves": run_moves_case}
+    cases = {"cost": run_cost_case, "exact_lut": run_exact_lut_case, "moves": run_moves_case, "lut": run_lut_case}
     out = cases[args.case](args, dev) if args.case in cases else run_ours(args, rank, world, dev)
     if rank == 0:
         print(json.dumps(out))

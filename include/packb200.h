@@ -275,6 +275,18 @@ int pk_relax(const float* xyt_in, const float* h_in, const int* offsets, const i
              const PkCostSpec* spec, const PkRelaxParams* params, float* xyt_out, float* h_out, float* loss_out,
              int* iters_out, float* work, void* stream);
 
+/* pk_relax on a part of the launch order: the count instances order[0 ..
+ * count-1] (order is required), with n_max bounding only their sizes and
+ * prm->threads sized for them; instances keep their indices 0 .. E-1 in
+ * every array, so several calls with disjoint parts of one largest-first
+ * order fill the same outputs and share one work buffer.  Launched on
+ * different streams, the parts -- size classes of a ragged batch, each with
+ * CTAs sized for its own trees -- run side by side.  Results equal
+ * pk_relax's bit for bit. */
+int pk_relax_ordered(const float* xyt_in, const float* h_in, const int* offsets, const int* order, int count, int E,
+                     int n_max, const PkCostSpec* spec, const PkRelaxParams* prm, float* xyt_out, float* h_out,
+                     float* loss_out, int* iters_out, float* work, void* stream);
+
 /* ---- serving: resumable device-resident relaxation jobs ---------------- */
 
 #define PK_JOB_NEW 0

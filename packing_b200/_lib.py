@@ -142,6 +142,8 @@ SIGNATURES = {
     "pk_wolfe_apply": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P],
     "pk_relax": [_P, _P, _P, _P, _I, _I, ctypes.POINTER(PkCostSpec), ctypes.POINTER(PkRelaxParams), _P, _P, _P,
                  _P, _P, _P],
+    "pk_relax_ordered": [_P, _P, _P, _P, _I, _I, _I, ctypes.POINTER(PkCostSpec), ctypes.POINTER(PkRelaxParams), _P,
+                         _P, _P, _P, _P, _P],
     "pk_relax_workspace_floats": [_P, _I, _I, _I],
     "pk_fma_probe": [_P, _I, _I, _I, _P],
     "pk_validate_fp64": [_P, _I, _I, _I, _P, _P, _P],

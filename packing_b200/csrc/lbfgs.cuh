@@ -561,22 +561,24 @@ __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const
     }
 }
 
-// One CTA per instance, or (persistent) one CTA per resident slot walking the
-// launch order with a stride of the grid: CTA b relaxes order[b],
-// order[b + G], ...; largest-first orders keep the CTAs' loads even.
+// One CTA per entry of the launch order (count entries), or (persistent) one
+// CTA per resident slot walking the order with a stride of the grid: CTA b
+// relaxes order[b], order[b + G], ...; largest-first orders keep the CTAs'
+// loads even.  Instances are indexed 0 .. E-1 whatever part of the order a
+// launch covers.
 template <int MODE, bool PERSISTENT, bool SYM>
 __global__ void __launch_bounds__(256, 3) pk_relax_kernel(const float* __restrict__ xyt_in, const float* __restrict__ h_in,
-                                const int* __restrict__ offsets, const int* __restrict__ order, int E, int n_max,
-                                PkCostSpec spec, PkRelaxParams prm, float* __restrict__ xyt_out,
+                                const int* __restrict__ offsets, const int* __restrict__ order, int count, int E,
+                                int n_max, PkCostSpec spec, PkRelaxParams prm, float* __restrict__ xyt_out,
                                 float* __restrict__ h_out, float* __restrict__ loss_out, int* __restrict__ iters_out,
                                 float* __restrict__ work, int cap_near, int cap_items)
 {
     extern __shared__ __align__(16) unsigned char pk_smem[];
-    if (!PERSISTENT) {
+    if (!PERSISTENT) {   // the grid is exactly count CTAs
         pk_relax_instance<MODE, SYM>(order ? order[blockIdx.x] : blockIdx.x, xyt_in, h_in, offsets, E, n_max, spec, prm,
                                 xyt_out, h_out, loss_out, iters_out, work, cap_near, cap_items, pk_smem);
     } else {
-        for (int k = blockIdx.x; k < E; k += gridDim.x) {
+        for (int k = blockIdx.x; k < count; k += gridDim.x) {
             pk_relax_instance<MODE, SYM>(order ? order[k] : k, xyt_in, h_in, offsets, E, n_max, spec, prm, xyt_out, h_out,
                                     loss_out, iters_out, work, cap_near, cap_items, pk_smem);
             __syncthreads();   // shared state is reused by the next instance
@@ -747,15 +749,19 @@ extern "C" size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_
     return 2 * (size_t)history * tot;
 }
 
-extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offsets, const int* order, int E,
-                        int n_max, const PkCostSpec* spec, const PkRelaxParams* prm, float* xyt_out, float* h_out,
-                        float* loss_out, int* iters_out, float* work, void* stream)
+// The launch behind pk_relax and pk_relax_ordered: count entries of the
+// launch order (all E instances when order is NULL).
+static int pk_relax_launch(const float* xyt_in, const float* h_in, const int* offsets, const int* order, int count,
+                           int E, int n_max, const PkCostSpec* spec, const PkRelaxParams* prm, float* xyt_out,
+                           float* h_out, float* loss_out, int* iters_out, float* work, void* stream)
 {
     int rc = pk_check_init();
     if (rc) return rc;
     if (!spec || !prm) return pk_fail(PK_EINVAL, "pk_relax: spec and params are required%s");
     if (E < 0 || n_max < 0) return pk_fail(PK_EINVAL, "pk_relax: negative size%s");
-    if (E == 0) return PK_OK;
+    if (count < 0 || count > E) return pk_fail(PK_EINVAL, "pk_relax: order count must be in [0, E]%s");
+    if (count < E && !order) return pk_fail(PK_EINVAL, "pk_relax: a partial launch needs an order%s");
+    if (E == 0 || count == 0) return PK_OK;
     if (n_max > PK_MAX_TREES) return pk_fail(PK_ERANGE, "pk_relax: more than 1024 trees per instance%s");
     if (prm->history < 1 || prm->history > 64) return pk_fail(PK_EINVAL, "pk_relax: history must be in [1, 64]%s");
     if (!xyt_in || !xyt_out || !loss_out || !work) return pk_fail(PK_EINVAL, "pk_relax: NULL pointer%s");
@@ -774,15 +780,16 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
     const size_t smem = pk_relax_smem_bytes(n_max, sym, cap_near, cap_items, prm->history);
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t err = cudaSuccess;
-    int grid = E;
+    int grid = count;
     switch (spec->pair_mode) {
 #define PK_R3(M, P, S)                                                                                   \
     {                                                                                                    \
         err = pk_set_smem((const void*)pk_relax_kernel<M, P, S>, 4 + M + 4 * (P) + 8 * (S), smem);      \
         if (err == cudaSuccess && (P))                                                                   \
-            err = pk_resident_grid((const void*)pk_relax_kernel<M, P, S>, T, smem, E, &grid);            \
+            err = pk_resident_grid((const void*)pk_relax_kernel<M, P, S>, T, smem, count, &grid);        \
         if (err == cudaSuccess)                                                                          \
-            pk_relax_kernel<M, P, S><<<grid, T, smem, st>>>(xyt_in, h_in, offsets, order, E, n_max, *spec, *prm, \
+            pk_relax_kernel<M, P, S><<<grid, T, smem, st>>>(xyt_in, h_in, offsets, order, count, E, n_max, *spec, \
+                                                            *prm,                                        \
                                                             xyt_out, h_out, loss_out, iters_out, work, cap_near, \
                                                             cap_items);                                  \
     }
@@ -804,6 +811,24 @@ extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offse
     }
     if (err != cudaSuccess) return pk_cuda_check(err, "pk_relax attribute");
     return pk_cuda_check(cudaGetLastError(), "pk_relax launch");
+}
+
+extern "C" int pk_relax(const float* xyt_in, const float* h_in, const int* offsets, const int* order, int E,
+                        int n_max, const PkCostSpec* spec, const PkRelaxParams* prm, float* xyt_out, float* h_out,
+                        float* loss_out, int* iters_out, float* work, void* stream)
+{
+    return pk_relax_launch(xyt_in, h_in, offsets, order, E, E, n_max, spec, prm, xyt_out, h_out, loss_out, iters_out,
+                           work, stream);
+}
+
+extern "C" int pk_relax_ordered(const float* xyt_in, const float* h_in, const int* offsets, const int* order,
+                                int count, int E, int n_max, const PkCostSpec* spec, const PkRelaxParams* prm,
+                                float* xyt_out, float* h_out, float* loss_out, int* iters_out, float* work,
+                                void* stream)
+{
+    if (!order) return pk_fail(PK_EINVAL, "pk_relax_ordered: order is required%s");
+    return pk_relax_launch(xyt_in, h_in, offsets, order, count, E, n_max, spec, prm, xyt_out, h_out, loss_out,
+                           iters_out, work, stream);
 }
 
 extern "C" int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* pool, int n_max, const PkCostSpec* spec,

@@ -5,9 +5,10 @@ One CUDA launch relaxes a whole batch: each CTA owns one packing, keeps its
 parameters ``x = [xyt (3n), h (3)]``, gradient and search direction in
 shared memory, evaluates the compound cost with the cost kernel's device code
 and runs all L-BFGS iterations without returning to the host.  Ragged
-batches (different tree counts) go in the same launch, largest first.  The
-launch is CUDA-graph capturable (no host synchronisation, no allocation
-inside ``relax_into``).
+batches (different tree counts) go largest first, either in one launch or as
+one launch per size class with CTAs sized for that class's trees, the
+classes side by side on forked streams.  ``relax_into`` does no host
+synchronisation and no allocation, so it can be captured in a CUDA graph.
 """
 from __future__ import annotations
 
@@ -65,11 +66,70 @@ def workspace_floats(sizes, history: int) -> int:
     return 2 * int(history) * sum(3 * int(s) + 3 for s in sizes)
 
 
+@dataclass(frozen=True)
+class SizeClass:
+    """A contiguous part of a largest-first launch order: ``count`` instances
+    from position ``start``, none with more than ``n_max`` trees, relaxed by
+    CTAs of ``threads`` threads (0: the library default for ``n_max``)."""
+    start: int
+    count: int
+    n_max: int
+    threads: int
+
+
+# (largest tree count, threads per CTA) of the size classes: a class's CTA
+# has a little more threads than its largest packing has trees, from 32 to
+# 256.  Chosen by timing class tables on a ragged batch of 8192 packings with
+# n log-uniform in [5, 200] (C4) on a B200.
+CLASS_TABLE = ((20, 32), (40, 64), (80, 96), (140, 160), (256, 256), (512, 256), (1024, 256))
+CLASS_EDGES = tuple(e for e, _ in CLASS_TABLE)
+
+
+def size_classes(sizes_in_order) -> list[SizeClass]:
+    """Size classes of a ragged batch, given its tree counts in the launch
+    order (largest first, as ``relax_ragged`` builds it).  A packing of n
+    trees goes to the class of the smallest edge >= n in ``CLASS_TABLE``,
+    whose CTAs have that entry's threads."""
+    sz = [int(v) for v in sizes_in_order]
+    if any(sz[k] < sz[k + 1] for k in range(len(sz) - 1)):
+        raise ValueError("sizes must be in a largest-first order")
+    out, k = [], 0
+    while k < len(sz):
+        edge = next((e for e in CLASS_EDGES if sz[k] <= e), None)
+        if edge is None:
+            raise ValueError(f"{sz[k]} trees exceeds {CLASS_EDGES[-1]}")
+        lo = max([e for e in CLASS_EDGES if e < edge], default=0)
+        j = k
+        while j < len(sz) and sz[j] > lo:
+            j += 1
+        out.append(SizeClass(start=k, count=j - k, n_max=sz[k], threads=dict(CLASS_TABLE)[edge]))
+        k = j
+    return out
+
+
+_side_streams: dict[int, list] = {}
+
+
+def _streams(dev, k):
+    d = _lib._dev_index(dev)
+    lst = _side_streams.setdefault(d, [])
+    while len(lst) < k:
+        lst.append(torch.cuda.Stream(device=torch.device("cuda", d)))
+    return lst[:k]
+
+
 def relax_into(xyt, h, xyt_out, h_out, loss_out, work, spec: CostSpec, params: RelaxParams, offsets=None,
-               order=None, n_max=None, iters_out=None, stream=None):
+               order=None, n_max=None, iters_out=None, stream=None, classes=None):
     """Launch the fused relaxation on caller-provided buffers (no host sync,
     no allocation).  Uniform: xyt (E, n, 3).  Ragged: xyt (sum n, 3) with
-    device int32 offsets (E+1,) and n_max."""
+    device int32 offsets (E+1,) and n_max.
+
+    ``classes`` (ragged, with a largest-first ``order``): a list of
+    ``SizeClass`` covering the order (``size_classes``).  Each class is one
+    ``pk_relax_ordered`` launch with CTAs sized for its own trees, on its own
+    stream forked from ``stream`` and joined back to it, so small packings
+    do not hold CTAs sized for the largest.  Results are the same bit for
+    bit as one launch."""
     x = _lib.as_tensor(xyt, "xyt")
     _lib.check_f32(x, "xyt")
     if offsets is None:
@@ -79,13 +139,43 @@ def relax_into(xyt, h, xyt_out, h_out, loss_out, work, spec: CostSpec, params: R
         nm = int(n_max)
     dev = x.device
     cs = spec.to_c()
-    ps = params.to_c()
+    L = _lib.load()
+    if classes is None:
+        ps = params.to_c()
+        with torch.cuda.device(dev):
+            rc = L.pk_relax(_lib.ptr(x), _lib.ptr(h), _lib.ptr(offsets), _lib.ptr(order), E, nm,
+                            ctypes.byref(cs), ctypes.byref(ps), _lib.ptr(xyt_out), _lib.ptr(h_out),
+                            _lib.ptr(loss_out), _lib.ptr(iters_out), _lib.ptr(work),
+                            ctypes.c_void_p(_lib.stream_handle(stream, dev)))
+        _lib.check(rc, "pk_relax")
+        return
+    if order is None or offsets is None:
+        raise ValueError("classes need a ragged batch with a largest-first order")
+    if sum(c.count for c in classes) != E or any(c.n_max > nm for c in classes):
+        raise ValueError("classes must cover the order once, each within n_max")
+    if stream is None:
+        base = torch.cuda.current_stream(dev)
+    elif isinstance(stream, torch.cuda.Stream):
+        base = stream
+    else:
+        base = torch.cuda.ExternalStream(_lib.stream_handle(stream, dev), device=dev)
+    side = _streams(dev, len(classes))
+    fork = torch.cuda.Event()
+    fork.record(base)
     with torch.cuda.device(dev):
-        rc = _lib.load().pk_relax(_lib.ptr(x), _lib.ptr(h), _lib.ptr(offsets), _lib.ptr(order), E, nm,
-                                  ctypes.byref(cs), ctypes.byref(ps), _lib.ptr(xyt_out), _lib.ptr(h_out),
-                                  _lib.ptr(loss_out), _lib.ptr(iters_out), _lib.ptr(work),
-                                  ctypes.c_void_p(_lib.stream_handle(stream, dev)))
-    _lib.check(rc, "pk_relax")
+        for c, st in zip(classes, side):
+            st.wait_event(fork)
+            ps = params.to_c()
+            ps.threads = int(c.threads)
+            rc = L.pk_relax_ordered(_lib.ptr(x), _lib.ptr(h), _lib.ptr(offsets),
+                                    ctypes.c_void_p(order.data_ptr() + 4 * c.start), c.count, E, c.n_max,
+                                    ctypes.byref(cs), ctypes.byref(ps), _lib.ptr(xyt_out), _lib.ptr(h_out),
+                                    _lib.ptr(loss_out), _lib.ptr(iters_out), _lib.ptr(work),
+                                    ctypes.c_void_p(st.cuda_stream))
+            _lib.check(rc, "pk_relax_ordered")
+            join = torch.cuda.Event()
+            join.record(st)
+            base.wait_event(join)
 
 
 def relax(xyt, h, spec: CostSpec = CostSpec(), params: RelaxParams = RelaxParams(), stream=None):
@@ -112,7 +202,9 @@ def relax(xyt, h, spec: CostSpec = CostSpec(), params: RelaxParams = RelaxParams
 
 
 def relax_ragged(xyt_list, h, spec: CostSpec = CostSpec(), params: RelaxParams = RelaxParams(), stream=None):
-    """Relax packings of different tree counts in ONE launch.  xyt_list: list
+    """Relax packings of different tree counts together, largest first:
+    one launch per size class (``size_classes``), side by side on forked
+    streams; with ``params.threads`` set, one launch for all.  xyt_list: list
     of (n_e, 3) CUDA tensors; h (E, 3).  Returns (list of relaxed (n_e, 3),
     h_out, loss (E,), iterations (E,))."""
     sizes = [int(a.shape[0]) for a in xyt_list]
@@ -126,14 +218,16 @@ def relax_ragged(xyt_list, h, spec: CostSpec = CostSpec(), params: RelaxParams =
     for s in sizes:
         off_h.append(off_h[-1] + s)
     offsets = torch.tensor(off_h, dtype=torch.int32, device=dev)
-    order = torch.tensor(sorted(range(E), key=lambda e: -sizes[e]), dtype=torch.int32, device=dev)
+    order_h = sorted(range(E), key=lambda e: -sizes[e])
+    order = torch.tensor(order_h, dtype=torch.int32, device=dev)
     hh = _lib.as_tensor(h, "h").contiguous() if h is not None else None
     xo = torch.empty_like(flat)
     ho = torch.empty_like(hh) if hh is not None else None
     loss = torch.empty(E, dtype=torch.float32, device=dev)
     iters = torch.empty(E, dtype=torch.int32, device=dev)
     work = torch.empty(max(1, workspace_floats(sizes, params.history_size)), dtype=torch.float32, device=dev)
+    classes = size_classes([sizes[e] for e in order_h]) if params.threads == 0 else None
     relax_into(flat, hh, xo, ho, loss, work, spec, params, offsets=offsets, order=order, n_max=max(sizes),
-               iters_out=iters, stream=stream)
+               iters_out=iters, stream=stream, classes=classes)
     outs = [xo[off_h[e]:off_h[e + 1]] for e in range(E)]
     return outs, ho, loss, iters

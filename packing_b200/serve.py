@@ -9,10 +9,12 @@ tree count and iteration budget are served continuously:
 * every admitted job keeps its poses, gradient and L-BFGS history resident in
   one device pool; admission is by memory footprint ((2 + 2m)(3n + 3) + m
   floats per job, first fit, FIFO);
-* each engine step launches ``pk_relax_jobs`` once over all resident jobs
-  (largest first) to advance each by ``chunk_iters`` iterations, then retires
-  finished jobs and admits waiting ones -- requests that arrive while others
-  run join at the next step and share launches with them;
+* each engine step advances every resident job by ``chunk_iters``
+  iterations with ``pk_relax_jobs``: the jobs go largest first, one launch
+  per size class (``relax.size_classes``: CTAs sized for that class's trees)
+  side by side on forked streams; then the step retires finished jobs and
+  admits waiting ones -- requests that arrive while others run join at the
+  next step and share launches with them;
 * a job's result does not depend on its neighbours or its chunking (order-
   fixed reductions, pause at iteration boundaries), so it equals the result
   of relaxing it alone.
@@ -33,7 +35,7 @@ import torch
 
 from . import _lib
 from .cost import CostSpec
-from .relax import RelaxParams
+from .relax import RelaxParams, SizeClass, _streams, size_classes
 
 
 @dataclass
@@ -84,7 +86,8 @@ class _Pool:
 
 class RelaxServer:
     def __init__(self, spec: CostSpec = CostSpec(), history: int = 10, max_step: float = 0.01,
-                 chunk_iters: int = 16, pool_floats: int = 1 << 27, max_jobs: int = 8192, device=None):
+                 chunk_iters: int = 16, pool_floats: int = 1 << 27, max_jobs: int = 8192, device=None,
+                 classes: bool = True):
         self.dev = torch.device(device or "cuda")
         _lib.ensure_init(self.dev)
         self.spec_c = spec.to_c()
@@ -105,6 +108,7 @@ class RelaxServer:
         self.launches = 0
         self._next_id = 0
         self.stream = torch.cuda.current_stream(self.dev)
+        self.classes = bool(classes)
 
     # ------------------------------------------------------------------
     def footprint(self, n: int) -> int:
@@ -126,6 +130,7 @@ class RelaxServer:
 
     def _admit(self):
         admitted = []
+        idx, vals = [], []
         while self.pending and self.free_slots:
             req = self.pending[0]
             need = self.footprint(req.xyt.shape[0])
@@ -140,10 +145,15 @@ class RelaxServer:
             J.n, J.max_iter, J.x_off, J.h_off = n, req.iters, off, off + 2 * N + self.m
             J.status, J.it, J.evals, J.hlen, J.hstart = _lib.PK_JOB_NEW, 0, 1, 0, 0
             J.H, J.loss, J.loss0 = 1.0, 0.0, 0.0
-            x = np.concatenate([req.xyt.reshape(-1), req.h]).astype(np.float32)
-            self.pool[off:off + N].copy_(torch.from_numpy(x), non_blocking=False)
+            idx.append(np.arange(off, off + N, dtype=np.int64))
+            vals.append(req.xyt.reshape(-1))
+            vals.append(req.h)
             self.resident[slot] = (req, off, need)
             admitted.append(slot)
+        if admitted:   # every admitted job's x = [xyt, h] in one copy and one scatter
+            ii = torch.from_numpy(np.concatenate(idx)).to(self.dev)
+            vv = torch.from_numpy(np.concatenate(vals).astype(np.float32)).to(self.dev)
+            self.pool.index_copy_(0, ii, vv)
         return admitted
 
     def step(self) -> list[Request]:
@@ -157,11 +167,24 @@ class RelaxServer:
         lst = torch.tensor(slots, dtype=torch.int32, device=self.dev)
         ctypes.memmove(self.table_pin.data_ptr(), ctypes.addressof(self.table_h), ctypes.sizeof(self.table_h))
         self.table_d.copy_(self.table_pin, non_blocking=True)
-        rc = _lib.load().pk_relax_jobs(ctypes.c_void_p(self.table_d.data_ptr()), _lib.ptr(lst), len(slots),
-                                       _lib.ptr(self.pool), n_max, ctypes.byref(self.spec_c),
-                                       ctypes.byref(self.prm_c), self.chunk,
-                                       ctypes.c_void_p(self.stream.cuda_stream))
-        _lib.check(rc, "pk_relax_jobs")
+        sizes = [self.resident[s][0].xyt.shape[0] for s in slots]
+        classes = size_classes(sizes) if self.classes else [SizeClass(0, len(slots), n_max, 0)]
+        side = _streams(self.dev, len(classes))
+        fork = torch.cuda.Event()
+        fork.record(self.stream)
+        L = _lib.load()
+        for c, st in zip(classes, side):
+            st.wait_event(fork)
+            prm = self.params.to_c()
+            prm.threads = int(c.threads)
+            rc = L.pk_relax_jobs(ctypes.c_void_p(self.table_d.data_ptr()),
+                                 ctypes.c_void_p(lst.data_ptr() + 4 * c.start), c.count, _lib.ptr(self.pool),
+                                 c.n_max, ctypes.byref(self.spec_c), ctypes.byref(prm), self.chunk,
+                                 ctypes.c_void_p(st.cuda_stream))
+            _lib.check(rc, "pk_relax_jobs")
+            join = torch.cuda.Event()
+            join.record(st)
+            self.stream.wait_event(join)
         self.launches += 1
         self.table_pin.copy_(self.table_d, non_blocking=True)
         self.stream.synchronize()
@@ -169,11 +192,17 @@ class RelaxServer:
         finished = [s for s in slots if self.table_h[s].status == _lib.PK_JOB_DONE]
         out = []
         if finished:
+            # every finished job's x = [xyt, h] in one gather and one copy
+            spans = [(self.resident[s][1], 3 * self.resident[s][0].xyt.shape[0] + 3) for s in finished]
+            ii = torch.from_numpy(np.concatenate([np.arange(o, o + k, dtype=np.int64) for o, k in spans]))
+            allx = self.pool.index_select(0, ii.to(self.dev)).cpu().numpy()
             now = time.perf_counter()
+            pos = 0
             for s in finished:
                 req, off, need = self.resident.pop(s)
                 n = req.xyt.shape[0]
-                x = self.pool[off:off + 3 * n + 3].cpu().numpy()
+                x = allx[pos:pos + 3 * n + 3]
+                pos += 3 * n + 3
                 req.result = x[:3 * n].reshape(n, 3).copy()
                 req.h_out = x[3 * n:].copy()
                 req.loss = float(self.table_h[s].loss)

@@ -108,3 +108,87 @@ def test_tuner_picks_feasible_shape_and_caches(cuda, tmp_path):
     prm = tn2.tuned(__import__("packing_b200.relax", fromlist=["RelaxParams"]).RelaxParams(history_size=5), 45,
                     _spec())
     assert prm.threads == t and prm.persistent == p
+
+
+def _ragged(cuda, sizes, seed=0):
+    flat = np.concatenate([poses(1, s, seed=seed + k)[0] for k, s in enumerate(sizes)]).astype(np.float32)
+    off = np.zeros(len(sizes) + 1, np.int32)
+    off[1:] = np.cumsum(sizes)
+    h = np.concatenate([square_h(1, s) for s in sizes]).astype(np.float32)
+    order_h = sorted(range(len(sizes)), key=lambda e: -sizes[e])
+    return (torch.from_numpy(flat).to(cuda), torch.from_numpy(h).to(cuda), torch.from_numpy(off).to(cuda),
+            torch.tensor(order_h, dtype=torch.int32, device=cuda), [sizes[e] for e in order_h])
+
+
+def test_size_classes_match_one_launch(cuda):
+    """One launch per size class, side by side on forked streams, gives the
+    bits of one launch for the whole ragged batch."""
+    from packing_b200.relax import RelaxParams, relax_into, size_classes, workspace_floats
+    rng = np.random.default_rng(8)
+    sizes = [int(s) for s in np.round(np.exp(rng.uniform(np.log(3), np.log(300), size=400)))]
+    xt, ht, offt, order, in_order = _ragged(cuda, sizes, seed=500)
+    prm = RelaxParams(n_iterations=30, history_size=5, max_step=0.01)
+    ref = _run(xt, ht, prm, offsets=offt, order=order, n_max=max(sizes))
+    classes = size_classes(in_order)
+    assert len(classes) >= 5
+    E = len(sizes)
+    xo, ho = torch.empty_like(xt), torch.empty_like(ht)
+    loss = torch.empty(E, device=cuda)
+    it = torch.empty(E, dtype=torch.int32, device=cuda)
+    work = torch.empty(workspace_floats(sizes, prm.history_size), device=cuda)
+    relax_into(xt, ht, xo, ho, loss, work, _spec(), prm, offsets=offt, order=order, n_max=max(sizes),
+               iters_out=it, classes=classes)
+    torch.cuda.synchronize()
+    for a, b in zip(ref, (xo.cpu().numpy(), loss.cpu().numpy(), it.cpu().numpy())):
+        assert np.array_equal(a, b)
+
+
+def test_size_classes_in_a_cuda_graph(cuda):
+    """The class launches and their stream fork / join captured in one CUDA
+    graph and replayed on new poses equal eager single launches."""
+    from packing_b200.relax import RelaxParams, relax_into, size_classes, workspace_floats
+    sizes = [7, 150, 33, 90, 12, 64, 200, 3, 48, 17] * 6
+    xt, ht, offt, order, in_order = _ragged(cuda, sizes, seed=900)
+    prm = RelaxParams(n_iterations=20, history_size=4, max_step=0.01)
+    classes = size_classes(in_order)
+    E = len(sizes)
+    xo, ho = torch.empty_like(xt), torch.empty_like(ht)
+    loss = torch.empty(E, device=cuda)
+    work = torch.empty(workspace_floats(sizes, prm.history_size), device=cuda)
+    side = torch.cuda.Stream(cuda)
+    side.wait_stream(torch.cuda.current_stream(cuda))
+    with torch.cuda.stream(side):   # warm-up off the capture
+        relax_into(xt, ht, xo, ho, loss, work, _spec(), prm, offsets=offt, order=order, n_max=max(sizes),
+                   classes=classes)
+    torch.cuda.current_stream(cuda).wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        relax_into(xt, ht, xo, ho, loss, work, _spec(), prm, offsets=offt, order=order, n_max=max(sizes),
+                   classes=classes)
+    for seed in (901, 902):
+        new, _, _, _, _ = _ragged(cuda, sizes, seed=seed)
+        xt.copy_(new)
+        g.replay()
+        torch.cuda.synchronize()
+        ref = _run(new, ht, prm, offsets=offt, order=order, n_max=max(sizes))
+        assert np.array_equal(xo.cpu().numpy(), ref[0])
+        assert np.array_equal(loss.cpu().numpy(), ref[1])
+    del g
+
+
+def test_partial_order_rejects_bad_counts(cuda):
+    import ctypes
+    from packing_b200 import _lib
+    from packing_b200.relax import RelaxParams
+    L = _lib.load()
+    cs, ps = _spec().to_c(), RelaxParams().to_c()
+    x = torch.zeros(30, device=cuda)
+    o = torch.zeros(4, dtype=torch.int32, device=cuda)
+    args = (_lib.ptr(x), _lib.ptr(x), None)
+    rc = L.pk_relax_ordered(*args, _lib.ptr(o), 5, 4, 10, ctypes.byref(cs), ctypes.byref(ps), _lib.ptr(x), None,
+                            _lib.ptr(x), None, _lib.ptr(x), None)
+    assert rc != 0   # count above E
+    rc = L.pk_relax_ordered(*args, None, 2, 4, 10, ctypes.byref(cs), ctypes.byref(ps), _lib.ptr(x), None,
+                            _lib.ptr(x), None, _lib.ptr(x), None)
+    assert rc != 0   # no order
