@@ -678,9 +678,14 @@ def run_lut_case(args, dev):
     T = np.linspace(-np.pi, np.pi, 360, dtype=np.float32)
     lut = LookupTable.build_from_kernel("area", X=X, Y=Y, theta=T, trim_zeros=False, device=dev)
     rng = np.random.default_rng(5)
-    E = args.lut_E
-    sizes = np.round(np.exp(rng.uniform(np.log(5), np.log(200), size=E))).astype(int)
-    xs = [workload(1, int(nn), seed=1000 + k)[0][0] for k, nn in enumerate(sizes)]
+    if args.lut_uniform:   # --E packings of --n trees instead of the C4 batch
+        E = args.E
+        sizes = np.full(E, args.n)
+        xs = list(workload(E, args.n, seed=0)[0])
+    else:
+        E = args.lut_E
+        sizes = np.round(np.exp(rng.uniform(np.log(5), np.log(200), size=E))).astype(int)
+        xs = [workload(1, int(nn), seed=1000 + k)[0][0] for k, nn in enumerate(sizes)]
     flat = torch.from_numpy(np.concatenate(xs)).to(dev)
     off = torch.tensor(np.concatenate([[0], np.cumsum(sizes)]), dtype=torch.int32, device=dev)
     nmax = int(sizes.max())
@@ -834,6 +839,8 @@ def main():
                          "moves: the GA's move selector on --ga-P rows of "
                          "--n trees (profiling captures)")
     ap.add_argument("--lut-n", dest="lut_n", type=int, default=900)
+    ap.add_argument("--lut-uniform", dest="lut_uniform", action="store_true",
+                    help="--case lut on --E packings of --n trees instead of the C4 batch")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
