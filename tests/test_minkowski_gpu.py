@@ -128,3 +128,15 @@ def test_forbidden_zone_has_no_holes(cuda):
         lab, n = ndimage.label(vals[:, :, k] < 0)
         edge = set(np.unique(np.concatenate([lab[0], lab[-1], lab[:, 0], lab[:, -1]]))) - {0}
         assert set(range(1, n + 1)) == edge, (k, float(T[k]), n, sorted(edge))
+
+
+def test_single_point_and_single_slice_grids(cuda):
+    """Grids of one point and of one slice (too few values for the share of
+    bit-identical entries to mean anything: tolerance and sign only)."""
+    T = np.array([0.7], np.float32)
+    for X, Y in ((np.array([0.1], np.float32), np.array([-0.05], np.float32)),
+                 (np.linspace(-0.3, 1.0, 9, dtype=np.float32),) * 2):
+        gpu, ora = _build(cuda, X, Y, T), MK.table(X, Y, T)
+        np.testing.assert_allclose(gpu, ora, rtol=0, atol=1e-6)
+        clear = np.abs(ora) > 1e-6
+        np.testing.assert_array_equal(gpu[clear] > 0, ora[clear] > 0)

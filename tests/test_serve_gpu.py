@@ -71,3 +71,19 @@ def test_trace_reports_latency(cuda):
     stats, done = srv.run_trace(reqs, arrivals)
     assert stats["requests"] == 40 and stats["p99_ms"] >= stats["p50_ms"] > 0
     assert all(r.iterations == r.iters for r in done)
+
+
+def test_size_classes_do_not_change_results(cuda):
+    """The engine's per-class launches give the bits of one launch over all
+    resident jobs."""
+    from packing_b200.serve import RelaxServer
+    jobs = [(n, 30 + (7 * n) % 90) for n in (3, 9, 17, 25, 41, 66, 85, 120, 150, 199, 200, 250)]
+    out = []
+    for classes in (True, False):
+        srv = RelaxServer(_spec(), history=5, chunk_iters=11, device=cuda, classes=classes)
+        reqs = [srv.submit(*_job(n, 300 + n), it) for n, it in jobs]
+        srv.drain()
+        out.append(reqs)
+    for a, b in zip(*out):
+        assert np.array_equal(a.result, b.result) and np.array_equal(a.h_out, b.h_out)
+        assert a.loss == b.loss and a.iterations == b.iterations
