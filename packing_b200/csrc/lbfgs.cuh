@@ -632,6 +632,9 @@ __global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict
     }
     if (threadIdx.x < m && resume) ro[threadIdx.x] = gx[2 * N + threadIdx.x];
     if (threadIdx.x < 3 && !resume) g[3 * n + threadIdx.x] = 0.f;
+    // a resumed job goes straight to the two-loop recursion, whose threads
+    // read elements of g and ro that other threads loaded
+    __syncthreads();
     PkRelaxVars v;
     v.it = J->it; v.evals = J->evals; v.hlen = J->hlen; v.hstart = J->hstart; v.active = 1;
     v.H = J->H; v.loss = J->loss; v.loss0 = J->loss0; v.ploss = 0.f; v.t = 0.f;
