@@ -111,6 +111,17 @@ typedef struct PkCostSpec {
 int pk_cost(const float* xyt, const int* offsets, int E, int n_uniform, const float* h,
             const PkCostSpec* spec, float* cost, float* grad, float* grad_h, void* stream);
 
+/* pk_cost on a part of a launch order: the count instances order[0 ..
+ * count-1] (order is required) of a batch of E, n_max bounding their
+ * sizes, threads per CTA (0: the default for n_max; else a multiple of 32 in
+ * [32, 256] with 8 * threads >= n_max - 1).  Instances keep their indices in
+ * every array, so calls with disjoint parts of one largest-first order --
+ * size classes of a ragged batch, on different streams -- fill the same
+ * outputs side by side.  Results equal pk_cost's bit for bit. */
+int pk_cost_ordered(const float* xyt, const int* offsets, const int* order, int count, int E, int n_max,
+                    const float* h, const PkCostSpec* spec, int threads, float* cost, float* grad, float* grad_h,
+                    void* stream);
+
 /* pack_cuda.overlap_multi_ensemble(xyt, xyt, use_separation, out_cost,
  * out_grads) (pack_cuda.py:1040-1183), non-periodic form. */
 int pk_overlap(const float* xyt, int E, int n, int use_separation, float* cost, float* grad,

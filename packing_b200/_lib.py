@@ -124,6 +124,7 @@ SIGNATURES = {
     "pk_init": [ctypes.POINTER(PkGeometry)],
     "pk_last_error": [],
     "pk_cost": [_P, _P, _I, _I, _P, ctypes.POINTER(PkCostSpec), _P, _P, _P, _P],
+    "pk_cost_ordered": [_P, _P, _P, _I, _I, _I, _P, ctypes.POINTER(PkCostSpec), _I, _P, _P, _P, _P],
     "pk_overlap": [_P, _I, _I, _I, _P, _P, _P],
     "pk_overlap_crystal": [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P],
     "pk_boundary": [_P, _P, _I, _I, _P, _P, _P, _P],

@@ -51,10 +51,12 @@ class CostSpec:
 
 
 def compound_cost(xyt, h, spec: CostSpec = CostSpec(), offsets=None, n_max=None, out_cost=None,
-                  out_grad=None, out_grad_h=None, evaluate_gradient=True, stream=None):
+                  out_grad=None, out_grad_h=None, evaluate_gradient=True, stream=None, order=None, classes=None):
     """Fused compound cost and gradient.  Uniform batch: ``xyt`` (E, n, 3).
     Ragged batch: ``xyt`` (sum n, 3) with int32 ``offsets`` (E+1,) on the
-    device and ``n_max`` >= every instance's tree count."""
+    device and ``n_max`` >= every instance's tree count; with a largest-first
+    ``order`` and its ``classes`` (``classes.ragged_plan``), one launch per
+    size class side by side, bit-identical to one launch."""
     x = _lib.as_tensor(xyt, "xyt")
     _lib.check_f32(x, "xyt")
     if offsets is None:
@@ -88,9 +90,31 @@ def compound_cost(xyt, h, spec: CostSpec = CostSpec(), offsets=None, n_max=None,
         return cost, grad, grad_h
     _lib.ensure_init(dev)
     cs = spec.to_c()
+    if classes is not None:
+        launch_cost_classes(x, off, order, E, nm, hh, cs, cost, grad, grad_h, classes, stream, "compound_cost")
+        return cost, grad, grad_h
     with torch.cuda.device(dev):
         rc = _lib.load().pk_cost(_lib.ptr(x), _lib.ptr(off), E, nm, _lib.ptr(hh), ctypes.byref(cs),
                                  _lib.ptr(cost), _lib.ptr(grad), _lib.ptr(grad_h),
                                  ctypes.c_void_p(_lib.stream_handle(stream, dev)))
     _lib.check(rc, "compound_cost")
     return cost, grad, grad_h
+
+
+def launch_cost_classes(x, off, order, E, n_max, h, cs, cost, grad, grad_h, classes, stream, what):
+    """One pk_cost_ordered launch per size class, side by side on forked streams."""
+    from .classes import launch_classes
+    if off is None or order is None:
+        raise ValueError(f"{what}: classes need a ragged batch with a largest-first order")
+    if sum(c.count for c in classes) != E or any(c.n_max > n_max for c in classes):
+        raise ValueError(f"{what}: classes must cover the order once, each within n_max")
+    L = _lib.load()
+
+    def launch(c, st):
+        rc = L.pk_cost_ordered(_lib.ptr(x), _lib.ptr(off), ctypes.c_void_p(order.data_ptr() + 4 * c.start), c.count,
+                               E, c.n_max, _lib.ptr(h), ctypes.byref(cs), int(c.threads), _lib.ptr(cost),
+                               _lib.ptr(grad), _lib.ptr(grad_h), ctypes.c_void_p(st))
+        _lib.check(rc, what)
+
+    with torch.cuda.device(x.device):
+        launch_classes(x.device, stream, classes, launch)

@@ -857,15 +857,17 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
     return total;
 }
 
+// CTA b costs instance order[b] (instance b without an order).
 template <int MODE, bool SYM>
-__global__ void __launch_bounds__(256, 3) pk_cost_kernel(const float* __restrict__ xyt, const int* __restrict__ offsets, int E,
+__global__ void __launch_bounds__(256, 3) pk_cost_kernel(const float* __restrict__ xyt, const int* __restrict__ offsets,
+                               const int* __restrict__ order, int E,
                                int n_max, const float* __restrict__ h, PkCostSpec spec,
                                float* __restrict__ cost, float* __restrict__ grad,
                                float* __restrict__ grad_h, int cap_near, int cap_items)
 {
     extern __shared__ __align__(16) unsigned char pk_smem[];
-    const int e = blockIdx.x;
-    if (e >= E) return;
+    const int e = order ? order[blockIdx.x] : blockIdx.x;
+    if (e < 0 || e >= E) return;
     const int base = offsets ? offsets[e] : e * n_max;
     const int n = offsets ? offsets[e + 1] - base : n_max;
     if (n < 0 || n > n_max) {
@@ -891,15 +893,19 @@ static inline int pk_cost_threads(int n_max)
 }
 
 
-static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max, const float* h,
-                          const PkCostSpec* spec, float* cost, float* grad, float* grad_h,
-                          cudaStream_t st)
+// count entries of the launch order (all E instances when order is NULL);
+// threads 0 = pk_cost_threads of the size bound.
+static int pk_launch_cost(const float* xyt, const int* offsets, const int* order, int count, int E, int n_max,
+                          const float* h, const PkCostSpec* spec, int threads, float* cost, float* grad,
+                          float* grad_h, cudaStream_t st)
 {
     int rc = pk_check_init();
     if (rc) return rc;
     if (!spec) return pk_fail(PK_EINVAL, "pk_cost: spec is NULL%s");
     if (E < 0 || n_max < 0) return pk_fail(PK_EINVAL, "pk_cost: negative size%s");
-    if (E == 0) return PK_OK;
+    if (count < 0 || count > E) return pk_fail(PK_EINVAL, "pk_cost: order count must be in [0, E]%s");
+    if (count < E && !order) return pk_fail(PK_EINVAL, "pk_cost: a partial launch needs an order%s");
+    if (E == 0 || count == 0) return PK_OK;
     if (spec && spec->symmetry != 0 && spec->symmetry != 1 && spec->symmetry != 2 && spec->symmetry != 4)
         return pk_fail(PK_EINVAL, "pk_cost: symmetry must be 0, 1, 2 or 4%s");
     if (n_max > PK_MAX_TREES || (spec && (long long)n_max * pk_symmetry(*spec) > PK_MAX_TREES))
@@ -912,7 +918,13 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
         if (!L.vals || L.nx < 2 || L.ny < 2 || L.nt < 2)
             return pk_fail(PK_EINVAL, "pk_cost: LUT needs vals and at least 2 points per axis%s");
     }
-    const int T = pk_cost_threads(n_max * pk_symmetry(*spec));
+    int T = pk_cost_threads(n_max * pk_symmetry(*spec));
+    if (threads != 0) {
+        if (threads < 32 || threads > 256 || (threads & 31) || 8 * threads < n_max * pk_symmetry(*spec) - 1)
+            return pk_fail(PK_EINVAL, "pk_cost: threads must be 0 or a multiple of 32 in [32, 256] with "
+                                      "8 * threads >= n - 1%s");
+        T = threads;
+    }
     int cap_near, cap_items;
     pk_caps(T, spec->pair_mode, &cap_near, &cap_items);
     const size_t smem = pk_cost_smem_bytes(n_max * pk_symmetry(*spec), cap_near, cap_items);
@@ -924,15 +936,15 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
             err = cudaFuncSetAttribute(pk_cost_kernel<M, true>,                                     \
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
             if (err == cudaSuccess)                                                                 \
-                pk_cost_kernel<M, true><<<E, T, smem, st>>>(xyt, offsets, E, n_max, h, *spec, cost, \
-                                                            grad, grad_h, cap_near, cap_items);     \
+                pk_cost_kernel<M, true><<<count, T, smem, st>>>(xyt, offsets, order, E, n_max, h, *spec, \
+                                                                cost, grad, grad_h, cap_near, cap_items); \
         } else {                                                                                    \
             err = cudaFuncSetAttribute(pk_cost_kernel<M, false>,                                    \
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
             if (err == cudaSuccess)                                                                 \
-                pk_cost_kernel<M, false><<<E, T, smem, st>>>(xyt, offsets, E, n_max, h, *spec,      \
-                                                             cost, grad, grad_h, cap_near,          \
-                                                             cap_items);                            \
+                pk_cost_kernel<M, false><<<count, T, smem, st>>>(xyt, offsets, order, E, n_max, h,    \
+                                                                 *spec, cost, grad, grad_h, cap_near, \
+                                                                 cap_items);                          \
         }                                                                                           \
         if (err == cudaSuccess) err = cudaGetLastError();                                           \
         break;
@@ -950,7 +962,17 @@ static int pk_launch_cost(const float* xyt, const int* offsets, int E, int n_max
 extern "C" int pk_cost(const float* xyt, const int* offsets, int E, int n_uniform, const float* h,
                        const PkCostSpec* spec, float* cost, float* grad, float* grad_h, void* stream)
 {
-    return pk_launch_cost(xyt, offsets, E, n_uniform, h, spec, cost, grad, grad_h, (cudaStream_t)stream);
+    return pk_launch_cost(xyt, offsets, nullptr, E, E, n_uniform, h, spec, 0, cost, grad, grad_h,
+                          (cudaStream_t)stream);
+}
+
+extern "C" int pk_cost_ordered(const float* xyt, const int* offsets, const int* order, int count, int E, int n_max,
+                               const float* h, const PkCostSpec* spec, int threads, float* cost, float* grad,
+                               float* grad_h, void* stream)
+{
+    if (!order) return pk_fail(PK_EINVAL, "pk_cost_ordered: order is required%s");
+    return pk_launch_cost(xyt, offsets, order, count, E, n_max, h, spec, threads, cost, grad, grad_h,
+                          (cudaStream_t)stream);
 }
 
 extern "C" int pk_overlap(const float* xyt, int E, int n, int use_separation, float* cost, float* grad,
@@ -960,7 +982,7 @@ extern "C" int pk_overlap(const float* xyt, int E, int n, int use_separation, fl
     memset(&s, 0, sizeof(s));
     s.pair_mode = use_separation ? PK_PAIR_SEP : PK_PAIR_AREA;
     s.w_pair = 1.f;
-    return pk_launch_cost(xyt, nullptr, E, n, nullptr, &s, cost, grad, nullptr, (cudaStream_t)stream);
+    return pk_launch_cost(xyt, nullptr, nullptr, E, E, n, nullptr, &s, 0, cost, grad, nullptr, (cudaStream_t)stream);
 }
 
 extern "C" int pk_boundary(const float* xyt, const float* h, int E, int n, float* cost, float* grad,
@@ -970,7 +992,7 @@ extern "C" int pk_boundary(const float* xyt, const float* h, int E, int n, float
     memset(&s, 0, sizeof(s));
     s.pair_mode = PK_PAIR_NONE;
     s.w_boundary = 1.f;
-    return pk_launch_cost(xyt, nullptr, E, n, h, &s, cost, grad, grad_h, (cudaStream_t)stream);
+    return pk_launch_cost(xyt, nullptr, nullptr, E, E, n, h, &s, 0, cost, grad, grad_h, (cudaStream_t)stream);
 }
 
 extern "C" int pk_overlap_lut(const float* xyt, const int* offsets, int E, int n_uniform, const PkLut* lut,
@@ -982,7 +1004,8 @@ extern "C" int pk_overlap_lut(const float* xyt, const int* offsets, int E, int n
     s.pair_mode = PK_PAIR_LUT;
     s.w_pair = 1.f;
     s.lut = *lut;
-    return pk_launch_cost(xyt, offsets, E, n_uniform, nullptr, &s, cost, grad, nullptr, (cudaStream_t)stream);
+    return pk_launch_cost(xyt, offsets, nullptr, E, E, n_uniform, nullptr, &s, 0, cost, grad, nullptr,
+                          (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -225,9 +225,12 @@ def overlap_multi_ensemble(xyt, out_cost, lut: LookupTable, out_grads=None, stre
 
 
 def overlap_multi_ensemble_ragged(xyt_packed, offsets, out_cost, lut: LookupTable, out_grads=None, n_max=None,
-                                  stream=None):
+                                  stream=None, order=None, classes=None):
     """Ragged form: ``xyt_packed`` (sum n, 3), int32 device ``offsets``
-    (E+1,), ``n_max`` >= every instance size (read from offsets if None)."""
+    (E+1,), ``n_max`` >= every instance size (read from offsets if None).
+    With a largest-first ``order`` and its ``classes``
+    (``classes.ragged_plan``): one launch per size class, side by side,
+    bit-identical to one launch."""
     x = _lib.as_tensor(xyt_packed, "xyt_packed")
     _lib.check_f32(x, "xyt_packed")
     off = _lib.as_tensor(offsets, "offsets")
@@ -246,6 +249,15 @@ def overlap_multi_ensemble_ragged(xyt_packed, offsets, out_cost, lut: LookupTabl
         return
     _lib.ensure_init(x.device)
     L = lut.c_struct()
+    if classes is not None:
+        from .cost import launch_cost_classes
+        cs = _lib.PkCostSpec()
+        cs.pair_mode = _lib.PK_PAIR_LUT
+        cs.w_pair = 1.0
+        cs.lut = L
+        launch_cost_classes(x, off, order, E, int(n_max), None, cs, c, g, None, classes, stream,
+                            "pack_cuda_lut.overlap_multi_ensemble_ragged")
+        return
     with torch.cuda.device(x.device):
         rc = _lib.load().pk_overlap_lut(_lib.ptr(x), _lib.ptr(off), E, int(n_max), ctypes.byref(L), _lib.ptr(c),
                                         _lib.ptr(g), ctypes.c_void_p(_lib.stream_handle(stream, x.device)))

@@ -18,6 +18,7 @@ from dataclasses import dataclass
 import torch
 
 from . import _lib
+from .classes import CLASS_EDGES, CLASS_TABLE, SizeClass, launch_classes, size_classes  # noqa: F401
 from .cost import CostSpec
 
 
@@ -66,58 +67,6 @@ def workspace_floats(sizes, history: int) -> int:
     return 2 * int(history) * sum(3 * int(s) + 3 for s in sizes)
 
 
-@dataclass(frozen=True)
-class SizeClass:
-    """A contiguous part of a largest-first launch order: ``count`` instances
-    from position ``start``, none with more than ``n_max`` trees, relaxed by
-    CTAs of ``threads`` threads (0: the library default for ``n_max``)."""
-    start: int
-    count: int
-    n_max: int
-    threads: int
-
-
-# (largest tree count, threads per CTA) of the size classes: a class's CTA
-# has a little more threads than its largest packing has trees, from 32 to
-# 256.  Chosen by timing class tables on a ragged batch of 8192 packings with
-# n log-uniform in [5, 200] (C4) on a B200.
-CLASS_TABLE = ((20, 32), (40, 64), (80, 96), (140, 160), (256, 256), (512, 256), (1024, 256))
-CLASS_EDGES = tuple(e for e, _ in CLASS_TABLE)
-
-
-def size_classes(sizes_in_order) -> list[SizeClass]:
-    """Size classes of a ragged batch, given its tree counts in the launch
-    order (largest first, as ``relax_ragged`` builds it).  A packing of n
-    trees goes to the class of the smallest edge >= n in ``CLASS_TABLE``,
-    whose CTAs have that entry's threads."""
-    sz = [int(v) for v in sizes_in_order]
-    if any(sz[k] < sz[k + 1] for k in range(len(sz) - 1)):
-        raise ValueError("sizes must be in a largest-first order")
-    out, k = [], 0
-    while k < len(sz):
-        edge = next((e for e in CLASS_EDGES if sz[k] <= e), None)
-        if edge is None:
-            raise ValueError(f"{sz[k]} trees exceeds {CLASS_EDGES[-1]}")
-        lo = max([e for e in CLASS_EDGES if e < edge], default=0)
-        j = k
-        while j < len(sz) and sz[j] > lo:
-            j += 1
-        out.append(SizeClass(start=k, count=j - k, n_max=sz[k], threads=dict(CLASS_TABLE)[edge]))
-        k = j
-    return out
-
-
-_side_streams: dict[int, list] = {}
-
-
-def _streams(dev, k):
-    d = _lib._dev_index(dev)
-    lst = _side_streams.setdefault(d, [])
-    while len(lst) < k:
-        lst.append(torch.cuda.Stream(device=torch.device("cuda", d)))
-    return lst[:k]
-
-
 def relax_into(xyt, h, xyt_out, h_out, loss_out, work, spec: CostSpec, params: RelaxParams, offsets=None,
                order=None, n_max=None, iters_out=None, stream=None, classes=None):
     """Launch the fused relaxation on caller-provided buffers (no host sync,
@@ -153,29 +102,18 @@ def relax_into(xyt, h, xyt_out, h_out, loss_out, work, spec: CostSpec, params: R
         raise ValueError("classes need a ragged batch with a largest-first order")
     if sum(c.count for c in classes) != E or any(c.n_max > nm for c in classes):
         raise ValueError("classes must cover the order once, each within n_max")
-    if stream is None:
-        base = torch.cuda.current_stream(dev)
-    elif isinstance(stream, torch.cuda.Stream):
-        base = stream
-    else:
-        base = torch.cuda.ExternalStream(_lib.stream_handle(stream, dev), device=dev)
-    side = _streams(dev, len(classes))
-    fork = torch.cuda.Event()
-    fork.record(base)
+
+    def launch(c, st):
+        ps = params.to_c()
+        ps.threads = int(c.threads)
+        rc = L.pk_relax_ordered(_lib.ptr(x), _lib.ptr(h), _lib.ptr(offsets),
+                                ctypes.c_void_p(order.data_ptr() + 4 * c.start), c.count, E, c.n_max,
+                                ctypes.byref(cs), ctypes.byref(ps), _lib.ptr(xyt_out), _lib.ptr(h_out),
+                                _lib.ptr(loss_out), _lib.ptr(iters_out), _lib.ptr(work), ctypes.c_void_p(st))
+        _lib.check(rc, "pk_relax_ordered")
+
     with torch.cuda.device(dev):
-        for c, st in zip(classes, side):
-            st.wait_event(fork)
-            ps = params.to_c()
-            ps.threads = int(c.threads)
-            rc = L.pk_relax_ordered(_lib.ptr(x), _lib.ptr(h), _lib.ptr(offsets),
-                                    ctypes.c_void_p(order.data_ptr() + 4 * c.start), c.count, E, c.n_max,
-                                    ctypes.byref(cs), ctypes.byref(ps), _lib.ptr(xyt_out), _lib.ptr(h_out),
-                                    _lib.ptr(loss_out), _lib.ptr(iters_out), _lib.ptr(work),
-                                    ctypes.c_void_p(st.cuda_stream))
-            _lib.check(rc, "pk_relax_ordered")
-            join = torch.cuda.Event()
-            join.record(st)
-            base.wait_event(join)
+        launch_classes(dev, stream, classes, launch)
 
 
 def relax(xyt, h, spec: CostSpec = CostSpec(), params: RelaxParams = RelaxParams(), stream=None):

@@ -11,7 +11,7 @@ tree count and iteration budget are served continuously:
   floats per job, first fit, FIFO);
 * each engine step advances every resident job by ``chunk_iters``
   iterations with ``pk_relax_jobs``: the jobs go largest first, one launch
-  per size class (``relax.size_classes``: CTAs sized for that class's trees)
+  per size class (``classes.size_classes``: CTAs sized for that class's trees)
   side by side on forked streams; then the step retires finished jobs and
   admits waiting ones -- requests that arrive while others run join at the
   next step and share launches with them;
@@ -35,7 +35,8 @@ import torch
 
 from . import _lib
 from .cost import CostSpec
-from .relax import RelaxParams, SizeClass, _streams, size_classes
+from .classes import SizeClass, launch_classes, size_classes
+from .relax import RelaxParams
 
 
 @dataclass
@@ -169,22 +170,17 @@ class RelaxServer:
         self.table_d.copy_(self.table_pin, non_blocking=True)
         sizes = [self.resident[s][0].xyt.shape[0] for s in slots]
         classes = size_classes(sizes) if self.classes else [SizeClass(0, len(slots), n_max, 0)]
-        side = _streams(self.dev, len(classes))
-        fork = torch.cuda.Event()
-        fork.record(self.stream)
         L = _lib.load()
-        for c, st in zip(classes, side):
-            st.wait_event(fork)
+
+        def launch(c, st):
             prm = self.params.to_c()
             prm.threads = int(c.threads)
             rc = L.pk_relax_jobs(ctypes.c_void_p(self.table_d.data_ptr()),
                                  ctypes.c_void_p(lst.data_ptr() + 4 * c.start), c.count, _lib.ptr(self.pool),
-                                 c.n_max, ctypes.byref(self.spec_c), ctypes.byref(prm), self.chunk,
-                                 ctypes.c_void_p(st.cuda_stream))
+                                 c.n_max, ctypes.byref(self.spec_c), ctypes.byref(prm), self.chunk, ctypes.c_void_p(st))
             _lib.check(rc, "pk_relax_jobs")
-            join = torch.cuda.Event()
-            join.record(st)
-            self.stream.wait_event(join)
+
+        launch_classes(self.dev, self.stream, classes, launch)
         self.launches += 1
         self.table_pin.copy_(self.table_d, non_blocking=True)
         self.stream.synchronize()

@@ -75,3 +75,33 @@ def test_lut_ragged_equals_uniform(cuda):
         pack_cuda_lut.overlap_multi_ensemble(xt, cu, lut, gu)
         assert float(cu[0]) == float(c[e])
         assert torch.equal(gu[0], g[o[e]:o[e + 1]])
+
+
+def test_ragged_size_classes_equal_one_launch(cuda):
+    """The ragged LUT cost and the ragged compound cost, launched per size
+    class side by side, give the bits of one launch."""
+    from packing_b200 import pack_cuda_lut
+    from packing_b200.classes import ragged_plan
+    from packing_b200.cost import CostSpec, compound_cost
+    lut = _small_lut(cuda, quad=True)
+    rng = np.random.default_rng(11)
+    sizes = [int(s) for s in np.round(np.exp(rng.uniform(np.log(2), np.log(260), size=300)))]
+    xs = [poses(1, s, seed=700 + k)[0] for k, s in enumerate(sizes)]
+    flat = torch.from_numpy(np.concatenate(xs)).to(cuda)
+    off = torch.tensor(np.concatenate([[0], np.cumsum(sizes)]), dtype=torch.int32, device=cuda)
+    order, classes = ragged_plan(sizes, cuda)
+    assert len(classes) >= 5
+    E = len(sizes)
+    c1, c2 = torch.empty(E, device=cuda), torch.empty(E, device=cuda)
+    g1, g2 = torch.empty_like(flat), torch.empty_like(flat)
+    pack_cuda_lut.overlap_multi_ensemble_ragged(flat, off, c1, lut, g1, n_max=max(sizes))
+    pack_cuda_lut.overlap_multi_ensemble_ragged(flat, off, c2, lut, g2, n_max=max(sizes), order=order,
+                                                classes=classes)
+    assert torch.equal(c1, c2) and torch.equal(g1, g2)
+    h = torch.from_numpy(np.concatenate([np.array([[np.sqrt(s * 0.2456875) * 1.3, 0, 0]], np.float32)
+                                         for s in sizes])).to(cuda)
+    spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=False)
+    a = compound_cost(flat, h, spec, offsets=off, n_max=max(sizes))
+    b = compound_cost(flat, h, spec, offsets=off, n_max=max(sizes), order=order, classes=classes)
+    for u, v in zip(a, b):
+        assert torch.equal(u, v)
