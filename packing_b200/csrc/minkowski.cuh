@@ -243,19 +243,26 @@ __global__ void __launch_bounds__(256) pk_mk_grid_kernel(const float* __restrict
     for (int tile = blockIdx.x; tile < tx * ty; tile += gridDim.x) {
         const int ix0 = (tile / ty) * PK_MK_TILE, iy0 = (tile % ty) * PK_MK_TILE;
         __syncthreads();   // the previous tile is done with rect, keep and hmask
-        if (threadIdx.x == 0) {
-            double4 r = make_double4(1e300, -1e300, 1e300, -1e300);
-            for (int i = ix0; i < ix0 + PK_MK_TILE && i < nx; ++i) {
-                r.x = fmin(r.x, (double)X[i]);
-                r.y = fmax(r.y, (double)X[i]);
+        if (threadIdx.x < 32) {
+            // lanes 0-15 read the tile's X values, lanes 16-31 its Y values;
+            // min and max within each half by shuffles
+            const int l = threadIdx.x & 15;
+            const bool isx = threadIdx.x < 16;
+            const int idx = (isx ? ix0 : iy0) + l;
+            const bool ok = idx < (isx ? nx : ny);
+            const double v = ok ? (double)(isx ? X[idx] : Y[idx]) : 0.0;
+            double lo = ok ? v : 1e300, hi = ok ? v : -1e300;
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) {
+                lo = fmin(lo, __shfl_xor_sync(PK_FULL_MASK, lo, o));
+                hi = fmax(hi, __shfl_xor_sync(PK_FULL_MASK, hi, o));
             }
-            for (int i = iy0; i < iy0 + PK_MK_TILE && i < ny; ++i) {
-                r.z = fmin(r.z, (double)Y[i]);
-                r.w = fmax(r.w, (double)Y[i]);
+            const double ylo = __shfl_sync(PK_FULL_MASK, lo, 16), yhi = __shfl_sync(PK_FULL_MASK, hi, 16);
+            if (threadIdx.x == 0) {
+                rect = make_double4(lo, hi, ylo, yhi);
+                nkeep = 0;
+                hmask = 0u;
             }
-            rect = r;
-            nkeep = 0;
-            hmask = 0u;
         }
         __syncthreads();
         const double4 r = rect;
