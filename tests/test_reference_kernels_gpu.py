@@ -118,6 +118,17 @@ def test_timing_against_reference_kernels(cuda):
         to = _time(lambda: pack_cuda.overlap_multi_ensemble(x, x, sep, out_cost=c, out_grads=g))
         lines.append(f"overlap {'sep ' if sep else 'area'} 4096 x n=200: reference {tr:.3f} ms, ours {to:.3f} ms, "
                      f"x{tr / to:.2f}")
+    from packing_b200 import pack_cuda_lut
+    from packing_b200.pack_cuda_lut import LookupTable
+    r0 = 0.5796198
+    X = np.linspace(-2 * r0, 2 * r0, 510, dtype=np.float32)[254:]
+    Y = np.linspace(-2 * r0, 2 * r0, 256, dtype=np.float32)
+    T = np.linspace(-np.pi, np.pi, 360, dtype=np.float32)
+    lut = LookupTable.build_from_kernel("area", X=X, Y=Y, theta=T, trim_zeros=False, device=cuda)
+    b = (lut.X_min, lut.X_max, lut.Y_min, lut.Y_max, lut.theta_min, lut.theta_max)
+    tr = _time(lambda: R.lut_overlap(x, lut.lut_d, b, False))
+    to = _time(lambda: pack_cuda_lut.overlap_multi_ensemble(x, c, lut, g))
+    lines.append(f"LUT 256 x 256 x 360, 4096 x n=200: reference {tr:.3f} ms, ours {to:.3f} ms, x{tr / to:.2f}")
     C = torch.rand((2048, 100, 100), device=cuda)
     tr = _time(lambda: R.hungarian(C), reps=3)
     to = _time(lambda: solve_lap_batch(C), reps=3)
