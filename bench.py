@@ -262,10 +262,13 @@ def run_ours(args, rank, world, dev):
                                 "(autotuned)",
                       "instances_stopped_early": stopped_early},
            "gpu_launches": args.steps, "clocks": clocks}
-    if rank != 0 or args.quick:
+    if args.quick:
         return out if rank == 0 else None
 
-    # ---- e2e through the public API, pinned host buffers ----
+    # ---- e2e through the public API, pinned host buffers: every rank at once,
+    # whole-job value over the slowest rank like the device-timed value ----
+    if world > 1:
+        torch.distributed.barrier()
     xyt_host = torch.from_numpy(xyt_np).pin_memory()
     h_host = torch.from_numpy(h_np).pin_memory()
     xo_host = torch.empty_like(xyt_host).pin_memory()
@@ -284,9 +287,18 @@ def run_ours(args, rank, world, dev):
         e1.synchronize()
         if k > 0:
             e2e_times.append(e0.elapsed_time(e1) / 1e3)
-    e2e = E * len(e2e_times) / sum(e2e_times)
-    out["e2e"] = {"value": e2e, "unit": "relaxations/s", "h2d_bytes_per_step": xyt_host.numel() * 4 + h_host.numel() * 4,
-                  "d2h_bytes_per_step": xo_host.numel() * 4 + loss_host.numel() * 4}
+    e2e_total = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+        torch.distributed.barrier()
+    e2e = E * world * len(e2e_times) / e2e_total
+    out["e2e"] = {"value": e2e, "unit": "relaxations/s",
+                  "h2d_bytes_per_step": world * (xyt_host.numel() * 4 + h_host.numel() * 4),
+                  "d2h_bytes_per_step": world * (xo_host.numel() * 4 + loss_host.numel() * 4)}
+    if rank != 0:
+        return None
 
     # ---- roofline: counted work of the same launch, FP32 SIMT peak ----
     counters = torch.zeros(6, dtype=torch.int64, device=dev)
