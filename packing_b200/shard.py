@@ -1,7 +1,7 @@
 """Instance sharding across GPUs (one process per GPU, torch.distributed).
 
 Packings are independent, so the path shards by instance with no collective
-in the data path (SURVEY of the reference: no distribution exists there).
+in the data path (the reference itself runs on one GPU and has no distribution).
 A GA generation needs one small exchange afterwards -- every rank learns the
 per-packing results (loss, square side, iterations) of all ranks -- which is
 one all_gather of a few floats per packing.
