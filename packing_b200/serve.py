@@ -180,7 +180,8 @@ class RelaxServer:
                                  c.n_max, ctypes.byref(self.spec_c), ctypes.byref(prm), self.chunk, ctypes.c_void_p(st))
             _lib.check(rc, "pk_relax_jobs")
 
-        launch_classes(self.dev, self.stream, classes, launch)
+        with torch.cuda.device(self.dev):
+            launch_classes(self.dev, self.stream, classes, launch)
         self.launches += 1
         self.table_pin.copy_(self.table_d, non_blocking=True)
         self.stream.synchronize()
