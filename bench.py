@@ -514,6 +514,30 @@ def measure_ragged_lut(args, dev):
     area_lut_spec = CostSpec(pair="lut", w_pair=1.0, w_boundary=1.0, w_area=0.0, fixed_h=True, lut=lut)
     relax_s = time_graph(area_lut_spec)
     single_s = time_relax(area_lut_spec, cls=None)
+
+    # the reference's grouping (pack_dynamics.py:177-183): one uniform launch per distinct n, one after another
+    groups = {}
+    for k, nn in enumerate(sizes):
+        groups.setdefault(int(nn), []).append(k)
+    gbufs = []
+    for nn, ks in groups.items():
+        xg = torch.from_numpy(np.stack([xs[k] for k in ks])).to(dev)
+        hg = torch.from_numpy(hs[ks]).to(dev)
+        gbufs.append((xg, hg, torch.empty_like(xg), torch.empty_like(hg), torch.empty(len(ks), device=dev),
+                      torch.empty(workspace_floats([nn] * len(ks), args.history), device=dev)))
+
+    def run_grouped():
+        for xg, hg, xgo, hgo, lg, wg in gbufs:
+            relax_into(xg, hg, xgo, hgo, lg, wg, area_lut_spec, prm)
+
+    run_grouped()
+    torch.cuda.synchronize(dev)
+    e0.record()
+    run_grouped()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    grouped_s = e0.elapsed_time(e1) / 1e3
+    del gbufs
     # LUT cost kernel alone: algorithmic bytes = 8 corners x 4 B per near pair
     cost = torch.empty(E, device=dev)
     grad = torch.empty_like(flat)
@@ -542,6 +566,7 @@ def measure_ragged_lut(args, dev):
             "launches": len(classes), "iterations": args.iters,
             "size_classes": [[c.n_max, c.count, c.threads] for c in classes],
             "single_launch_relaxations_per_s": E / single_s,
+            "grouped_by_n_relaxations_per_s": E / grouped_s, "grouped_by_n_launches": len(groups),
             "lut_cost_kernel_ms": lut_ms,
             "lut_kernel_algorithmic_GBps": near_total * 32 / (lut_ms * 1e-3) / 1e9,
             "note": "largest first, one launch per size class (n_max, count, threads per CTA) side by side on "
@@ -583,6 +608,21 @@ def measure_ga_step(args, dev):
     e1.record()
     torch.cuda.synchronize(dev)
     lap_ms = e0.elapsed_time(e1) / 3
+    # the reference's diversity metric as a second matrix family (kaggle_support.py:2107-2112)
+    mates = pop[partners]
+    dd = pop[:, :, None, :2] - mates[:, None, :, :2]
+    dt = torch.remainder(pop[:, :, None, 2] - mates[:, None, :, 2] + np.pi, 2 * np.pi) - np.pi
+    C2 = torch.sqrt((dd * dd).sum(-1) + dt * dt).to(torch.float32).contiguous()
+    del dd, dt
+    lap_batch.solve_lap_batch(C2)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(3):
+        lap_batch.solve_lap_batch(C2)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    lap2_ms = e0.elapsed_time(e1) / 3
+    hbm_peak, hbm_src = measured_hbm_gbps()
     crossover_jitter_step(pop, partners, hh, gen, iterations=args.ga_iters)
     torch.cuda.synchronize(dev)
     e0.record()
@@ -617,8 +657,13 @@ def measure_ga_step(args, dev):
     torch.cuda.synchronize(dev)
     ref_ms = e0.elapsed_time(e1)
     counts = torch.bincount(chosen[chosen >= 0].long(), minlength=len(moves.moves)).cpu().tolist()
+    lap_bytes = P * n * n * 4 + P * n * 8
     return {"population": P, "n": n, "lap_instances_per_s": P / (lap_ms * 1e-3), "lap_ms": lap_ms,
-            "lap_hbm_GBps": P * n * n * 4 / (lap_ms * 1e-3) / 1e9, "generation_ms": step_ms,
+            "lap_hbm_GBps": lap_bytes / (lap_ms * 1e-3) / 1e9,
+            "lap_hbm_frac": lap_bytes / (lap_ms * 1e-3) / 1e9 / hbm_peak, "lap_hbm_peak_source": hbm_src,
+            "lap_reference_metric_ms": lap2_ms,
+            "lap_reference_metric": "sqrt(dx^2 + dy^2 + wrap(dtheta)^2), kaggle_support.py:2107-2112",
+            "generation_ms": step_ms,
             "generations_per_s": 1e3 / step_ms, "relax_iterations": args.ga_iters,
             "reference_ga_offspring": {
                 "moves_ms": moves_ms, "moves_rows_per_s": P / (moves_ms * 1e-3),
