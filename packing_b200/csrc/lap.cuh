@@ -47,14 +47,20 @@ __device__ __forceinline__ bool pk_hungarian_warp(int N, float* u, int* rm, Cost
                     if (minv[k] < lbv) { lbv = minv[k]; lbj = j; }
                 }
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const float ov = __shfl_xor_sync(PK_FULL_MASK, lbv, o);
-                const int oj = __shfl_xor_sync(PK_FULL_MASK, lbj, o);
-                if (ov < lbv || (ov == lbv && oj < lbj)) { lbv = ov; lbj = oj; }
+            // Warp argmin in two redux.sync steps: the smallest slack as an
+            // order-preserving unsigned key (-0 folded into +0, so equal
+            // floats give equal keys), then the lowest column among the
+            // lanes holding it.  Slacks are never NaN: a NaN cost fails the
+            // '<' above and leaves minv untouched.
+            {
+                const unsigned bits = __float_as_uint(__fadd_rn(lbv, 0.f));
+                const unsigned key = (bits & 0x80000000u) ? ~bits : (bits | 0x80000000u);
+                const unsigned kmin = __reduce_min_sync(PK_FULL_MASK, key);
+                lbj = (int)__reduce_min_sync(PK_FULL_MASK, key == kmin ? (unsigned)lbj : 0xffffffffu);
             }
             if (lbj == 0x7fffffff) return false;   // no finite slack: infeasible input
-            const float delta = lbv;
+            // the winning lane's own slack, bit for bit
+            const float delta = __shfl_sync(PK_FULL_MASK, lbv, lbj & 31);
 #pragma unroll
             for (int k = 0; k < CPL; ++k) {
                 const int j = lane + 32 * k;
