@@ -12,6 +12,8 @@
 #include "common.cuh"
 
 #define PK_LAP_WARPS 4
+// dynamic shared memory one CTA may hold on sm_100a (227 KB)
+#define PK_LAP_SMEM_MAX ((size_t)227 * 1024)
 
 // Warp-cooperative Hungarian for problem b.  u and rm are this warp's shared
 // arrays of N entries.  costfn(row, col) returns C[row][col] for this
@@ -137,9 +139,97 @@ pk_hungarian_kernel(const float* __restrict__ C, int B, int N, int* __restrict__
     }
 }
 
+// The same solver with the problem's N x N costs copied into shared memory
+// first.  Each Dijkstra step reads one cost row, and which row is only known
+// when the previous step ends, so every step waits a full load latency: from
+// shared memory that wait is a few tens of cycles instead of an L2 round trip.
+// One warp per CTA; the CTAs beyond those resident start as others finish,
+// which balances problems of very different step counts.
+template <int CPL>
+__global__ void __launch_bounds__(32)
+pk_hungarian_smem_kernel(const float* __restrict__ C, int B, int N, int* __restrict__ row_match,
+                         float* __restrict__ total, int* __restrict__ status)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    const int lane = threadIdx.x;
+    const int b = blockIdx.x;
+    if (b >= B) return;
+    const size_t nn = (size_t)N * N;
+    float* Cs = (float*)pk_smem;
+    float* u = Cs + ((nn + 3) & ~(size_t)3);
+    int* rm = (int*)(u + N);
+    const float* Cb = C + (size_t)b * nn;
+    if ((((uintptr_t)Cb) & 15) == 0) {
+        const size_t n4 = nn >> 2;
+        const float4* src = (const float4*)Cb;
+        float4* dst = (float4*)Cs;
+#pragma unroll 8
+        for (size_t k = lane; k < n4; k += 32) dst[k] = __ldg(src + k);
+        for (size_t k = (n4 << 2) + lane; k < nn; k += 32) Cs[k] = __ldg(Cb + k);
+    } else {
+        for (size_t k = lane; k < nn; k += 32) Cs[k] = __ldg(Cb + k);
+    }
+    __syncwarp();
+    const bool ok = pk_hungarian_warp<CPL>(N, u, rm, [&](int r, int j) { return Cs[r * N + j]; });
+    __syncwarp();
+    for (int r = lane; r < N; r += 32) row_match[(size_t)b * N + r] = ok ? rm[r] : -1;
+    if (lane == 0) {
+        float t = 0.f;
+        if (ok) {
+            for (int r = 0; r < N; ++r) {
+                const int col = rm[r];
+                if (col >= 0 && col < N) t += Cs[r * N + col];
+            }
+        } else {
+            t = __int_as_float(0x7fc00000);
+        }
+        total[b] = t;
+        if (status) status[b] = ok ? 0 : 1;
+    }
+}
+
+// Shared memory of the staged solver for N: the matrix (rounded up to whole
+// float4s), u and the row matches.
+static size_t pk_lap_smem_bytes(int N)
+{
+    return (((size_t)N * N + 3) & ~(size_t)3) * 4 + (size_t)N * 8;
+}
+
+// Launches the staged solver when every problem can be resident at once
+// (staging trades concurrency for latency: with fewer problems in flight
+// than the SMs could hold from L2, the L2 form finishes first).  Returns 1
+// if launched, 0 if the L2 form should run, or a status on failure.
+template <int CPL>
+static int pk_lap_try_smem(const float* C, int B, int N, int* rm, float* tot, int* status, cudaStream_t st)
+{
+    const size_t ssm = pk_lap_smem_bytes(N);
+    if (ssm > PK_LAP_SMEM_MAX) return 0;
+    cudaError_t err = cudaFuncSetAttribute(pk_hungarian_smem_kernel<CPL>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm);
+    int dev = 0, sms = 0, per_sm = 0;
+    if (err == cudaSuccess) err = cudaGetDevice(&dev);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (err == cudaSuccess)
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk_hungarian_smem_kernel<CPL>, 32, ssm);
+    if (err != cudaSuccess) return pk_cuda_check(err, "pk_lap_solve occupancy");
+    if ((long long)per_sm * sms < (long long)B) return 0;
+    pk_hungarian_smem_kernel<CPL><<<B, 32, ssm, st>>>(C, B, N, rm, tot, status);
+    const int rc = pk_cuda_check(cudaGetLastError(), "pk_lap_solve launch");
+    return rc == PK_OK ? 1 : rc;
+}
+
 static int pk_lap_dispatch(const float* C, int B, int N, int* rm, float* tot, int* status, cudaStream_t st)
 {
     const int cpl = (N + 31) / 32;
+    int staged = 0;
+    switch (cpl) {
+#define PK_L(K) case K: staged = pk_lap_try_smem<K>(C, B, N, rm, tot, status, st); break;
+        PK_L(1) PK_L(2) PK_L(3) PK_L(4) PK_L(5) PK_L(6) PK_L(7) PK_L(8)
+#undef PK_L
+        default: return pk_fail(PK_ERANGE, "pk_lap_solve: N beyond 256%s");
+    }
+    if (staged == 1) return PK_OK;
+    if (staged != 0) return staged;
     const dim3 grid((B + PK_LAP_WARPS - 1) / PK_LAP_WARPS), block(32 * PK_LAP_WARPS);
     const size_t smem = (size_t)PK_LAP_WARPS * 2 * N * 4;
     switch (cpl) {

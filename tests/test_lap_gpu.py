@@ -26,6 +26,28 @@ def test_random_bitexact(cuda, N):
     assert np.array_equal(tot.view(np.int32), otot.view(np.int32))
 
 
+def test_staged_and_l2_forms_bitexact(cuda):
+    """The solver stages each matrix in shared memory when every problem of
+    the batch can be resident at once (600 of 100 x 100 on a B200), and
+    reads it from L2 otherwise (1000): both give the oracle's answer.  An odd
+    side and a base one float past a 16-byte boundary take the scalar copy."""
+    rng = np.random.default_rng(5)
+    for B, N in ((600, 100), (1000, 100), (9, 37)):
+        C = rng.random((B, N, N)).astype(np.float32)
+        rm, tot = _solve(C, cuda)
+        orm, otot = O.hungarian(C)
+        assert np.array_equal(rm, orm)
+        assert np.array_equal(tot.view(np.int32), otot.view(np.int32))
+    from packing_b200.lap_batch import solve_lap_batch
+    flat = rng.random(1 + 7 * 36 * 36).astype(np.float32)
+    view = torch.from_numpy(flat).to(cuda)[1:].view(7, 36, 36)
+    assert view.data_ptr() % 16 != 0
+    rm, tot = solve_lap_batch(view)
+    orm, otot = O.hungarian(flat[1:].reshape(7, 36, 36))
+    assert np.array_equal(rm.cpu().numpy(), orm)
+    assert np.array_equal(tot.cpu().numpy(), otot)
+
+
 def test_ties_bitexact(cuda):
     """Integer costs with many equal slacks: ties must go to the lowest column."""
     rng = np.random.default_rng(1)
