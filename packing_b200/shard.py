@@ -11,6 +11,10 @@ ranges (work ~ n^2 per packing: the pair enumeration and the near pairs grow
 with n^2 at fixed density).  ``gather_results(local, counts, group)``
 all-gathers per-instance rows of the shards into the global order.
 ``relax_shard(...)`` relaxes this rank's range with the fused kernel.
+``gather_champions(xyt, fitness, offset, k, group)`` gives every rank the
+same k best packings of the whole population (the reference set of the GA's
+diversity matching, ``kaggle_support.py:2014-2129``) from one all_gather of
+each rank's own k best.
 """
 from __future__ import annotations
 
@@ -70,3 +74,49 @@ def relax_shard(xyt_list, h, spec, params, rank: int, world: int, device=None, g
     else:
         table = local
     return table, outs, (s, e)
+
+
+def gather_champions(xyt: torch.Tensor, fitness: torch.Tensor, offset: int, k: int, group=None):
+    """The k packings of lowest fitness over all ranks, identical on every rank.
+
+    xyt: (E_local, n, 3) this rank's packings (n equal on every rank);
+    fitness: (E_local,); offset: global index of this rank's first packing.
+    Each rank offers its own k best (ties to the lower global index), so one
+    all_gather of k rows of (fitness, global index, n * 3 poses) in float64
+    carries every candidate; the global selection uses the same order.
+    Returns (xyt (k', n, 3) in xyt's dtype, fitness (k',) float64, global
+    indices (k',) int64), k' = min(k, population size), best first.
+    """
+    if xyt.dim() != 3 or xyt.shape[2] != 3:
+        raise ValueError("xyt must be (E_local, n, 3)")
+    if fitness.shape != (xyt.shape[0],):
+        raise ValueError("fitness must be (E_local,)")
+    if k < 0:
+        raise ValueError("k must be >= 0")
+    E, n = xyt.shape[0], xyt.shape[1]
+    dev = xyt.device
+    fit = fitness.to(torch.float64)
+    gidx = torch.arange(offset, offset + E, dtype=torch.float64, device=dev)
+
+    def best(f, g, m):
+        # lexicographic (fitness, global index): sort by index, then a stable sort by fitness
+        o = torch.argsort(g, stable=True)
+        o = o[torch.argsort(f[o], stable=True)]
+        return o[:m]
+
+    pick = best(fit, gidx, min(k, E))
+    rows = torch.full((k, 2 + 3 * n), float("nan"), dtype=torch.float64, device=dev)
+    rows[:, 0] = float("inf")
+    rows[:, 1] = -1.0
+    m = pick.numel()
+    rows[:m, 0] = fit[pick]
+    rows[:m, 1] = gidx[pick]
+    rows[:m, 2:] = xyt[pick].reshape(m, 3 * n).to(torch.float64)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        parts = [torch.empty_like(rows) for _ in range(dist.get_world_size(group))]
+        dist.all_gather(parts, rows, group=group)
+        rows = torch.cat(parts, 0)
+    rows = rows[rows[:, 1] >= 0]
+    sel = best(rows[:, 0], rows[:, 1], min(k, rows.shape[0]))
+    out = rows[sel]
+    return (out[:, 2:].reshape(-1, n, 3).to(xyt.dtype), out[:, 0].clone(), out[:, 1].to(torch.int64))

@@ -69,3 +69,50 @@ def test_gather_results_two_ranks_gloo():
         assert np.array_equal(t[:, 1], np.array(sizes) * 0.5)
         owner = np.concatenate([[k] * (b - a) for k, (a, b) in enumerate(ranges)])
         assert np.array_equal(t[:, 2], owner)
+
+
+def _champ_worker(rank, world, port, q):
+    from packing_b200.shard import gather_champions
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        xyt, fit = _champ_population()
+        ranges = [(0, 3), (3, 11)]   # rank 0 holds fewer packings than k
+        s, e = ranges[rank]
+        q.put((rank, [t.numpy() for t in gather_champions(xyt[s:e], fit[s:e], s, 5)]))
+    finally:
+        dist.destroy_process_group()
+
+
+def _champ_population():
+    g = torch.Generator().manual_seed(3)
+    xyt = torch.rand((11, 4, 3), generator=g)
+    fit = torch.tensor([0.5, 0.2, 0.9, 0.2, 0.7, 0.1, 0.2, 0.8, 0.3, float("inf"), 0.05])
+    return xyt, fit
+
+
+def test_gather_champions_two_ranks_gloo():
+    """Every rank gets the same k best packings, ties to the lower global
+    index, equal to selecting from the whole population in one process."""
+    from packing_b200.shard import gather_champions
+    xyt, fit = _champ_population()
+    ref = gather_champions(xyt, fit, 0, 5)
+    assert ref[2].tolist() == [10, 5, 1, 3, 6]
+    assert torch.equal(ref[0], xyt[ref[2]])
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_champ_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in range(2):
+        for a, b in zip(out[r], ref):
+            assert np.array_equal(a, b.numpy())
+    # fewer packings than k in the whole population
+    few = gather_champions(xyt[:2], fit[:2], 0, 5)
+    assert few[2].tolist() == [1, 0]
