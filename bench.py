@@ -153,7 +153,7 @@ FLOPS_PER_ITER_ELEM = 12
 # launch, from a one-pass ncu capture of that launch, per (E, n, iterations,
 # history); other configurations report null.  Almost all of it is the final
 # write-back of the L-BFGS history (2 m (3n + 3) floats per packing).
-TRAFFIC_BYTES = {(4096, 200, 200, 10): 344.6e6}
+TRAFFIC_BYTES = {(4096, 200, 200, 10): 183.1e6}
 HBM_FALLBACK_GBPS = 6650.0
 
 

@@ -506,6 +506,23 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
     }
 }
 
+// Drops the 128-byte L2 lines wholly inside [p, p + nbytes) without writing
+// them back (PTX discard.global.L2).  A one-shot relaxation's history is
+// scratch of its launch: without this, every finished packing's 2 m N floats
+// stay dirty in L2 and are written to HBM when later packings evict them
+// (315 MB per 4096 x n = 200 launch at m = 10).  A line shared with the
+// neighbouring packing's history is left alone.  The caller has synchronised
+// the block after the last access; the region's contents are undefined
+// afterwards, and every history slot is written before it is read.
+__device__ __forceinline__ void pk_discard_l2(const void* p, size_t nbytes)
+{
+    const size_t g = __cvta_generic_to_global(p);
+    const size_t b = (g + 127) & ~(size_t)127;
+    const size_t e = (g + nbytes) & ~(size_t)127;
+    for (size_t a = b + (size_t)threadIdx.x * 128; a < e; a += (size_t)blockDim.x * 128)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(a) : "memory");
+}
+
 // Relaxes instance e (all threads of the block call it; e is uniform).
 template <int MODE, bool SYM>
 __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const float* __restrict__ h_in,
@@ -548,6 +565,7 @@ __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const
     pk_relax_iterate<MODE, SYM>(x, g, pg, d, al, ro, red, flip, S, Y, n, h_in != nullptr, spec, prm, sm, v, false,
                            prm.max_iter, hist_streamed);
     __syncthreads();
+    pk_discard_l2(S, (size_t)2 * m * N * sizeof(float));
     for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) xyt_out[(size_t)base * 3 + k] = x[k];
     if (h_out && threadIdx.x < 3) h_out[3 * e + threadIdx.x] = x[3 * n + threadIdx.x];
     if (threadIdx.x == 0) {
