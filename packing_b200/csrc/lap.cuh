@@ -322,11 +322,25 @@ __device__ __forceinline__ float3 pk_div_transform(float x, float y, float th, i
     return make_float3(nx, ny, __fsub_rn(m, PI));
 }
 
+// fmodf(x, 2 pi) (2 pi rounded to float), exactly: |x| < 2 pi is its own
+// remainder, and for 2 pi <= |x| < 4 pi the remainder |x| - 2 pi is exact
+// (Sterbenz) and takes the sign of x; anything else goes to fmodf.  The
+// cost rows of the fused diversity solver are generated inside its Dijkstra
+// steps, where the general fmodf was most of a step's arithmetic.
+__device__ __forceinline__ float pk_fmod_2pi(float x)
+{
+    const float T = 2.f * 3.14159265358979323846f;
+    const float ax = fabsf(x);
+    if (ax < T) return x;
+    if (ax < 2.f * T) return copysignf(__fsub_rn(ax, T), x);
+    return fmodf(x, T);
+}
+
 __device__ __forceinline__ float pk_div_cost(float px, float py, float pt, float3 r)
 {
     const float PI = 3.14159265358979323846f;
     const float dx = __fsub_rn(px, r.x), dy = __fsub_rn(py, r.y);
-    float dt = fmodf(__fadd_rn(__fsub_rn(pt, r.z), PI), 2.f * PI);
+    float dt = pk_fmod_2pi(__fadd_rn(__fsub_rn(pt, r.z), PI));
     if (dt < 0.f) dt = __fadd_rn(dt, 2.f * PI);
     dt = __fsub_rn(dt, PI);
     return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dt, dt)));

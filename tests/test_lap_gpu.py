@@ -139,6 +139,57 @@ def test_genetic_diversity_matrix(cuda):
         np.testing.assert_allclose(M[t * 12:(t + 1) * 12].cpu().numpy(), C64, rtol=1e-5, atol=1e-5)
 
 
+def _diversity_costs_f32(P, R):
+    """The diversity cost matrices (kaggle_support.py:2061-2112, torch float32:
+    remainder = fmod, plus the divisor when the sign differs) restated in
+    float32 numpy with the kernel's rounding order, stacked (transform, pop,
+    ref) -> (n, n)."""
+    f = np.float32
+    PI = f(np.pi)
+    T = f(2) * PI
+    ca, sa = [f(1), f(0), f(-1), f(0)], [f(0), f(1), f(0), f(-1)]
+    ang = [f(0), f(1.5707963267948966), f(3.141592653589793), f(4.71238898038469)]
+
+    def rem(x):
+        m = np.fmod(x, T)
+        return np.where(m < 0, m + T, m)
+
+    out = []
+    for t in range(8):
+        x, y, th = R[..., 0], R[..., 1], R[..., 2]
+        if t >= 4:
+            y, th = -y, PI - th
+        r = t & 3
+        if r:
+            x, y = x * ca[r] - y * sa[r], x * sa[r] + y * ca[r]
+            th = th + ang[r]
+        th = rem(th + PI) - PI
+        dx = P[:, None, :, None, 0] - x[None, :, None, :]
+        dy = P[:, None, :, None, 1] - y[None, :, None, :]
+        dt = rem((P[:, None, :, None, 2] - th[None, :, None, :]) + PI) - PI
+        out.append(np.sqrt((dx * dx + dy * dy) + dt * dt).astype(f))
+    return np.stack(out).reshape(-1, P.shape[1], P.shape[1])
+
+
+def test_diversity_costs_bitexact_wide_angles(cuda):
+    """Cost matrices equal the float32 restatement bit for bit for angles far
+    outside [0, 2 pi) as well, so every branch of the kernel's remainder
+    (|x| < 2 pi, 2 pi <= |x| < 4 pi, beyond) meets the general fmod."""
+    from packing_b200.lap_batch import genetic_diversity_cost_matrices, genetic_diversity_matrix, solve_lap_batch
+    rng = np.random.default_rng(17)
+    P = poses(3, 40, seed=21)
+    R = poses(2, 40, seed=22)
+    P[..., 2] = rng.uniform(-25.0, 25.0, P.shape[:2])
+    R[..., 2] = rng.uniform(-25.0, 25.0, R.shape[:2])
+    P[0, :4, 2] = [0.0, -0.0, np.float32(2 * np.pi), -np.float32(4 * np.pi)]
+    M = genetic_diversity_cost_matrices(torch.from_numpy(P).to(cuda), torch.from_numpy(R).to(cuda)).cpu().numpy()
+    ref = _diversity_costs_f32(P.astype(np.float32), R.astype(np.float32))
+    assert np.array_equal(M.view(np.int32), ref.view(np.int32))
+    D = genetic_diversity_matrix(torch.from_numpy(P).to(cuda), torch.from_numpy(R).to(cuda)).cpu().numpy()
+    _, tot = solve_lap_batch(torch.from_numpy(ref).to(cuda))
+    assert np.array_equal(D, tot.reshape(8, 3, 2).amin(0).cpu().numpy())
+
+
 def test_diversity_shortcut(cuda):
     from packing_b200.lap_batch import compute_diversity_shortcut_kernel
     pop = poses(5, 40, seed=13)
