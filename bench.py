@@ -872,6 +872,38 @@ def run_moves_case(args, dev):
             "algorithmic_GBps": algo / (ms * 1e-3) / 1e9}
 
 
+def run_lap_case(args, dev):
+    """Batched Hungarian on --ga-P matrices of n = --n trees: squared centre
+    distance + |wrapped angle difference| between seeded packings and
+    shuffled partners, as the matched crossover builds them; --warmup then
+    --steps solves timed with CUDA events.  Algorithmic bytes: the matrices
+    read once plus the row matches and totals written.  A profiling case, not
+    a benchmark metric."""
+    import torch
+
+    from packing_b200 import lap_batch
+    from packing_b200.ga_step import matching_costs
+    P, n = args.ga_P, args.n
+    xyt, _ = workload(P, n, seed=21)
+    pop = torch.from_numpy(xyt).to(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    C = matching_costs(pop, pop[torch.randperm(P, generator=g, device=dev)])
+    for _ in range(args.warmup):
+        lap_batch.solve_lap_batch(C)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        lap_batch.solve_lap_batch(C)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    algo = P * n * n * 4.0 + P * n * 4.0 + P * 4.0
+    return {"case": "lap", "problems": P, "n": n, "ms_per_solve": ms, "problems_per_s": P / (ms * 1e-3),
+            "algorithmic_GBps": algo / (ms * 1e-3) / 1e9}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -926,7 +958,7 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline timing only")
     ap.add_argument("--no-tune", dest="no_tune", action="store_true",
                     help="default launch shape instead of the autotuned one (profiling captures)")
-    ap.add_argument("--case", default="relax", choices=["relax", "cost", "exact_lut", "moves", "lut"],
+    ap.add_argument("--case", default="relax", choices=["relax", "cost", "exact_lut", "moves", "lut", "lap"],
                     help="relax: the headline; cost: the compound cost kernel alone on E packings, at the "
                          "initial poses and after --iters iterations of relaxation; exact_lut: the exact-separation "
                          "table build on --lut-n points per axis; lut: the LUT cost kernel alone on the C4 batch; "
@@ -953,7 +985,8 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=dev)
-    cases = {"cost": run_cost_case, "exact_lut": run_exact_lut_case, "moves": run_moves_case, "lut": run_lut_case}
+    cases = {"cost": run_cost_case, "exact_lut": run_exact_lut_case, "moves": run_moves_case, "lut": run_lut_case,
+             "lap": run_lap_case}
     out = cases[args.case](args, dev) if args.case in cases else run_ours(args, rank, world, dev)
     if rank == 0:
         print(json.dumps(out))
