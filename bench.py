@@ -123,6 +123,30 @@ def fp32_peak_tflops(torch, L, dev):
     return best
 
 
+def gather_peak(torch, L, table, dev):
+    """Measured trilinear lookups per second on uniformly random cells of
+    ``table`` (nx, ny, nt) -- the LUT itself, so the same size and L2
+    residency -- best of 5: the ceiling of the LUT cost kernel."""
+    import ctypes
+    props = torch.cuda.get_device_properties(dev)
+    blocks, threads, iters = props.multi_processor_count * 8, 256, 32
+    nx, ny, nt = (int(v) for v in table.shape)
+    out = torch.empty(blocks, device=dev)
+    st = torch.cuda.current_stream(dev)
+    best = 0.0
+    for k in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        rc = L.pk_gather_probe(ctypes.c_void_p(table.data_ptr()), nx, ny, nt, ctypes.c_void_p(out.data_ptr()),
+                               blocks, threads, iters, 7 + k, ctypes.c_void_p(st.cuda_stream))
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        assert rc == 0
+        if k:
+            best = max(best, blocks * threads * iters * 2 / (e0.elapsed_time(e1) * 1e-3))
+    return best
+
+
 def cpu_baseline_relax(E, n, iters, history, seed=123):
     """The FP64 oracle relaxing a bounded sample of the same workload."""
     from oracle import oracle as O
@@ -440,6 +464,18 @@ def measure_serve(args, dev):
                         f"{hist}, max_step 0.01, boundary + overlap area"}
 
 
+def lut_gather_roofline(lookups_per_s, lut, dev):
+    """The LUT cost kernel's trilinear lookups per second against the measured
+    ceiling of lookups on random cells of the same table."""
+    import torch
+
+    from packing_b200 import _lib
+    peak = gather_peak(torch, _lib.load(), lut.lut_d, dev)
+    return {"achieved_lookups_per_s": lookups_per_s, "peak_lookups_per_s": peak, "frac": lookups_per_s / peak,
+            "peak_source": "measured: 8-corner lookups on uniformly random cells of the same table "
+                           "(pk_gather_probe)"}
+
+
 def measure_ragged_lut(args, dev):
     """8192 instances, n log-uniform in [5, 200], LUT 256 x 256 x 360 built
     from the overlap-area kernel; one launch relaxes them all.  The same batch
@@ -569,6 +605,7 @@ def measure_ragged_lut(args, dev):
             "grouped_by_n_relaxations_per_s": E / grouped_s, "grouped_by_n_launches": len(groups),
             "lut_cost_kernel_ms": lut_ms,
             "lut_kernel_algorithmic_GBps": near_total * 32 / (lut_ms * 1e-3) / 1e9,
+            "lut_gather_roofline": lut_gather_roofline(near_total / (lut_ms * 1e-3), lut, dev),
             "note": "largest first, one launch per size class (n_max, count, threads per CTA) side by side on "
                     "forked streams, captured once in a CUDA graph and replayed per step; LUT tabulates the "
                     "overlap area",
@@ -799,6 +836,7 @@ def run_lut_case(args, dev):
         near += int(((d ** 2).sum(-1) <= (2 * 0.5796198) ** 2).sum() - len(x)) // 2
     return {"case": "lut", "instances": E, "lut_shape": list(lut.lut_d.shape), "ms_per_launch": ms,
             "near_pairs": near, "lookups_per_s": near / (ms * 1e-3),
+            "gather_roofline": lut_gather_roofline(near / (ms_cls * 1e-3), lut, dev),
             "algorithmic_GBps": near * 32 / (ms * 1e-3) / 1e9, "checksum": float(cost.double().sum()),
             "size_classes": {"ms": ms_cls, "launches": len(classes), "lookups_per_s": near / (ms_cls * 1e-3),
                              "algorithmic_GBps": near * 32 / (ms_cls * 1e-3) / 1e9}}

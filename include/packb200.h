@@ -443,6 +443,12 @@ size_t pk_relax_workspace_floats(const int* sizes_host, int E, int n_uniform, in
  * roofline denominator of the SIMT-bound kernels. */
 int pk_fma_probe(float* out, int blocks, int threads, int iters, void* stream);
 
+/* Trilinear-lookup probe: blocks x threads x iters x 2 lookups, each the 8
+ * corner loads of a random cell of the C-ordered (nx, ny, nt) float table, for
+ * the roofline denominator of the LUT kernel (lookups per second). */
+int pk_gather_probe(const float* table, int nx, int ny, int nt, float* out, int blocks, int threads, int iters,
+                    unsigned seed, void* stream);
+
 int pk_version(void);
 
 #ifdef __cplusplus

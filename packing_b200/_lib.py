@@ -147,6 +147,7 @@ SIGNATURES = {
                          _P, _P, _P, _P, _P],
     "pk_relax_workspace_floats": [_P, _I, _I, _I],
     "pk_fma_probe": [_P, _I, _I, _I, _P],
+    "pk_gather_probe": [_P, _I, _I, _I, _P, _I, _I, _I, ctypes.c_uint, _P],
     "pk_validate_fp64": [_P, _I, _I, _I, _P, _P, _P],
     "pk_snap": [_P, _P, _I, _I, _P, _P, _P],
     "pk_relax_jobs": [_P, _P, _I, _P, _I, ctypes.POINTER(PkCostSpec), ctypes.POINTER(PkRelaxParams), _I, _P],

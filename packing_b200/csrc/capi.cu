@@ -38,3 +38,41 @@ extern "C" int pk_fma_probe(float* out, int blocks, int threads, int iters, void
     pk_fma_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(out, iters);
     return pk_cuda_check(cudaGetLastError(), "pk_fma_probe launch");
 }
+
+// Trilinear-lookup probe: the LUT kernel's access pattern on uniformly random
+// cells.  Each thread runs 2 independent xorshift streams; every step of a
+// stream picks a cell (ix < nx - 1, iy < ny - 1, it < nt - 1) of the
+// C-ordered (nx, ny, nt) table and loads its 8 corners.  Lookups per second
+// on the LUT itself (same size, same L2 residency) are the measured ceiling
+// the LUT cost kernel's lookups are compared with.
+__global__ void pk_gather_probe_kernel(const float* __restrict__ t, int nx, int ny, int nt, float* out, int iters,
+                                       unsigned seed)
+{
+    unsigned x[2];
+    const unsigned id = blockIdx.x * blockDim.x + threadIdx.x;
+    x[0] = (id * 2u + 1u) * 0x9E3779B9u ^ seed;
+    x[1] = (id * 2u + 2u) * 0x9E3779B9u ^ seed;
+    const size_t sy = (size_t)nt, sx = (size_t)ny * nt;
+    float acc = 0.f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            x[k] ^= x[k] << 13; x[k] ^= x[k] >> 17; x[k] ^= x[k] << 5;
+            const unsigned ix = x[k] % (unsigned)(nx - 1), iy = (x[k] >> 8) % (unsigned)(ny - 1),
+                           it = (x[k] >> 16) % (unsigned)(nt - 1);
+            const float* c = t + ix * sx + iy * sy + it;
+            acc += __ldg(c) + __ldg(c + 1) + __ldg(c + sy) + __ldg(c + sy + 1) + __ldg(c + sx) + __ldg(c + sx + 1)
+                   + __ldg(c + sx + sy) + __ldg(c + sx + sy + 1);
+        }
+    }
+    if (acc == 12345.678f) out[blockIdx.x] = acc;   // keeps the loads alive
+}
+
+extern "C" int pk_gather_probe(const float* table, int nx, int ny, int nt, float* out, int blocks, int threads,
+                               int iters, unsigned seed, void* stream)
+{
+    if (!table || !out || nx < 2 || ny < 2 || nt < 2 || blocks < 1 || threads < 1 || threads > 1024 || iters < 1)
+        return pk_fail(PK_EINVAL, "pk_gather_probe: bad arguments%s");
+    pk_gather_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(table, nx, ny, nt, out, iters, seed);
+    return pk_cuda_check(cudaGetLastError(), "pk_gather_probe launch");
+}

@@ -78,6 +78,36 @@ def test_dropin_fp32_packing_matches_oracle(cuda):
     np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=0, atol=2e-4)
 
 
+def test_headline_sampled_instances_track_fp64_oracle(cuda):
+    """16 packings sampled evenly from the 4096 x n = 200 headline batch (same
+    seeded poses, m = 10, max_step 0.01, boundary + overlap area, fixed side):
+    20 iterations of the fused FP32 relaxation follow the FP64 oracle's
+    relaxation (C cost restatement + numpy lbfgs restatement).  Measured on a
+    B200: poses within 3.6e-5, losses within 7.9e-6 relative.  Further out the
+    two trajectories of this nonsmooth cost separate (1e-2 relative at 50
+    iterations), as any two precisions would."""
+    from packing_b200.cost import CostSpec
+    from packing_b200.relax import RelaxParams, relax
+    idx = np.linspace(0, 4095, 16).astype(int)
+    xyt = poses(4096, 200, seed=0)[idx]
+    h = square_h(16, 200)
+    E, n = xyt.shape[:2]
+    spec = CostSpec(pair="area", w_pair=1.0, w_boundary=1.0, w_area=1e-2, fixed_h=True)
+
+    def fo(xx):
+        c, g, gh = O.compound_cost(xx[:, :3 * n].reshape(E, n, 3), xx[:, 3 * n:], w_area=1e-2, fixed_h=True)
+        return c, np.concatenate([g.reshape(E, -1), gh], 1)
+
+    x0 = np.concatenate([xyt.reshape(E, -1), h], 1).astype(np.float64)
+    xo, _ = O.lbfgs(fo, x0, max_iter=20, history_size=10, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+    co, _ = fo(xo)
+    xr, hr, loss, it = relax(torch.from_numpy(xyt).to(cuda), torch.from_numpy(h).to(cuda), spec,
+                             RelaxParams(n_iterations=20, history_size=10, max_step=0.01))
+    assert torch.all(it == 20)
+    np.testing.assert_allclose(xr.cpu().numpy().reshape(E, -1), xo[:, :3 * n], rtol=0, atol=2e-4)
+    np.testing.assert_allclose(loss.cpu().numpy(), co, rtol=5e-5)
+
+
 def test_fused_relax_matches_dropin(cuda):
     """The one-launch relaxation and the drop-in lbfgs over the same kernel
     cost follow the same iterates bit for bit (both use order-fixed
