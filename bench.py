@@ -175,8 +175,9 @@ FLOPS_PER_ITER_ELEM = 12
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one relaxation
 # launch, from a one-pass ncu capture of that launch, per (E, n, iterations,
-# history); other configurations report null.  Almost all of it is the final
-# write-back of the L-BFGS history (2 m (3n + 3) floats per packing).
+# history); other configurations report null.  Most of it is L-BFGS history
+# (2 m (3n + 3) floats per packing) written back from L2 while packings run;
+# a finished packing's history is discarded from L2, not written back.
 TRAFFIC_BYTES = {(4096, 200, 200, 10): 183.1e6}
 HBM_FALLBACK_GBPS = 6650.0
 
@@ -585,6 +586,19 @@ def measure_ragged_lut(args, dev):
     e1.record()
     torch.cuda.synchronize(dev)
     lut_ms = e0.elapsed_time(e1) / 10
+    # and one launch per size class, the form the relaxation above uses
+    from packing_b200.classes import ragged_plan
+    order_c, classes_c = ragged_plan(sizes.tolist(), dev)
+    pack_cuda_lut.overlap_multi_ensemble_ragged(flat, off, cost, lut, grad, n_max=nmax, order=order_c,
+                                                classes=classes_c)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(10):
+        pack_cuda_lut.overlap_multi_ensemble_ragged(flat, off, cost, lut, grad, n_max=nmax, order=order_c,
+                                                    classes=classes_c)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    lut_cls_ms = e0.elapsed_time(e1) / 10
     near = 0
     for k in range(0, E, max(1, E // 256)):      # sampled near-pair count
         xk = xs[k]
@@ -605,7 +619,9 @@ def measure_ragged_lut(args, dev):
             "grouped_by_n_relaxations_per_s": E / grouped_s, "grouped_by_n_launches": len(groups),
             "lut_cost_kernel_ms": lut_ms,
             "lut_kernel_algorithmic_GBps": near_total * 32 / (lut_ms * 1e-3) / 1e9,
-            "lut_gather_roofline": lut_gather_roofline(near_total / (lut_ms * 1e-3), lut, dev),
+            "lut_cost_kernel_classes_ms": lut_cls_ms,
+            "lut_kernel_classes_algorithmic_GBps": near_total * 32 / (lut_cls_ms * 1e-3) / 1e9,
+            "lut_gather_roofline": lut_gather_roofline(near_total / (lut_cls_ms * 1e-3), lut, dev),
             "note": "largest first, one launch per size class (n_max, count, threads per CTA) side by side on "
                     "forked streams, captured once in a CUDA graph and replayed per step; LUT tabulates the "
                     "overlap area",
