@@ -1016,8 +1016,8 @@ def main():
                     help="relax: the headline; cost: the compound cost kernel alone on E packings, at the "
                          "initial poses and after --iters iterations of relaxation; exact_lut: the exact-separation "
                          "table build on --lut-n points per axis; lut: the LUT cost kernel alone on the C4 batch; "
-                         "moves: the GA's move selector on --ga-P rows of "
-                         "--n trees (profiling captures)")
+                         "moves: the GA's move selector on --ga-P rows of --n trees; lap: the batched Hungarian on "
+                         "--ga-P matched-crossover matrices of --n trees (profiling captures)")
     ap.add_argument("--lut-n", dest="lut_n", type=int, default=900)
     ap.add_argument("--lut-uniform", dest="lut_uniform", action="store_true",
                     help="--case lut on --E packings of --n trees instead of the C4 batch")
