@@ -53,3 +53,13 @@ def test_errors_are_codes_not_crashes():
     assert rc == -4
     assert b"256" in L.pk_last_error()
     assert L.pk_relax_workspace_floats(None, 10, 200, 10) == 2 * 10 * 10 * 603
+
+
+def test_probes_reject_bad_arguments_before_launching():
+    """The roofline probes validate their arguments on the host and return a
+    status (no launch, so this runs without a device)."""
+    L = _lib.load()
+    assert L.pk_gather_probe(None, 256, 256, 360, None, 1, 1, 1, 0, None) != 0
+    assert b"pk_gather_probe" in L.pk_last_error()
+    assert L.pk_fma_probe(None, 1, 1, 1, None) != 0
+    assert b"pk_fma_probe" in L.pk_last_error()
