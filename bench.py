@@ -751,7 +751,23 @@ def measure_legalize(args, dev):
     dt = time.perf_counter() - t0
     legal = r.legal.cpu().numpy()
     side = r.side.cpu().numpy()
-    return {"packings": E, "n": n, "accepted_fp64": int(legal.sum()),
+    # the FP64 validator alone on the legalised packings tiled to 4096: accepted
+    # packings have no overlapping pair, so every near pair runs all its tests
+    from packing_b200.validate import validate
+    big = r.xyt.repeat(max(1, 4096 // E), 1, 1).contiguous()
+    validate(big)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        validate(big)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    vms = e0.elapsed_time(e1) / 5
+    validator = {"packings": int(big.shape[0]), "n": n, "ms": vms, "packings_per_s": big.shape[0] / (vms * 1e-3),
+                 "what": "pk_validate_fp64 (FP64 side + separating-axis legality) on the legalised packings, "
+                         f"tiled {max(1, 4096 // E)}x"}
+    return {"packings": E, "n": n, "accepted_fp64": int(legal.sum()), "validator": validator,
             "side_mean_accepted": float(side[legal].mean()) if legal.any() else None,
             "rounds_max": int(r.rounds.max()), "seconds": dt,
             "schedule": "snap, then up to 20 rounds: area weight 1e-2 halved, max_step 1e-4 x sqrt(1/2)^k, "
