@@ -192,6 +192,159 @@ def measured_hbm_gbps():
         return HBM_FALLBACK_GBPS, "fallback"
 
 
+def reference_lbfgs():
+    """The reference's own batched L-BFGS (core/lbfgs_torch_parallel.py:411-729),
+    imported unmodified from the reference package that baseline/install_ref.py
+    installs into baseline/_ref (torch only).  None when it is not installed."""
+    import importlib.util
+    path = os.path.join(ROOT, "baseline", "_ref", "core", "lbfgs_torch_parallel.py")
+    if not os.path.exists(path):
+        return None
+    spec = importlib.util.spec_from_file_location("reference_lbfgs_torch_parallel", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.lbfgs
+
+
+def run_simulation_plain(lbfgs_ref, cost_fn, xyt, h, iters, hist):
+    """OptimizerBFGS.run_simulation's flow (pack_dynamics.py:73-137) with torch
+    in place of cupy: x = [xyt, h] flattened per packing, an objective that
+    unflattens through persistent buffers, evaluates the cost terms and
+    flattens the gradients into a fresh array (:95-124), and the reference's
+    lbfgs with pack_dynamics' arguments (tolerances 0, no line search).
+    cost_fn(xyt, h, cost, grad, grad_h) fills the three outputs."""
+    import torch
+    E, n = int(xyt.shape[0]), int(xyt.shape[1])
+    ns = 3 * n
+    x0 = torch.cat([xyt.reshape(E, -1), h], 1).contiguous()
+    tmp_x = torch.zeros_like(x0)
+    tmp_xyt = xyt.clone()
+    tmp_h = h.clone()
+    tmp_cost = torch.zeros(E, device=xyt.device)
+    tmp_grad = torch.zeros_like(xyt)
+    tmp_grad_h = torch.zeros_like(h)
+
+    def f_torch(x, is_main_loop):
+        M = x.shape[0]
+        tmp_x[:M] = x
+        tmp_xyt[:M] = tmp_x[:M, :ns].reshape(M, -1, 3)
+        tmp_h[:M] = tmp_x[:M, ns:]
+        cost_fn(tmp_xyt[:M], tmp_h[:M], tmp_cost[:M], tmp_grad[:M], tmp_grad_h[:M])
+        res = torch.zeros_like(tmp_x[:M])
+        res[:, :ns] = tmp_grad[:M].reshape(M, -1)
+        res[:, ns:] = tmp_grad_h[:M]
+        return tmp_cost[:M], res
+
+    lbfgs_ref(f_torch, x0, tolerance_grad=0, tolerance_change=0, tolerance_rel_change=0.0, max_iter=iters,
+              history_size=hist, max_step=0.01, line_search_fn=None, stop_on_cost_increase=False)
+    return x0, tmp_cost
+
+
+def time_plain(torch, dev, lbfgs_ref, cost_fn, xyt, h, iters, hist):
+    """One warm-up relaxation of 3 iterations, then one full relaxation timed
+    with CUDA events on the current stream (the host loop's syncs included)."""
+    run_simulation_plain(lbfgs_ref, cost_fn, xyt, h, 3, hist)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    x, cost = run_simulation_plain(lbfgs_ref, cost_fn, xyt, h, iters, hist)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) / 1e3, x, cost
+
+
+def measure_plain_reference(args, dev, xyt, h, spec, fused_value, fused_loss):
+    """The plain forms of the north star's comparison, on the same GPU:
+    P (plain_reference_lbfgs): this package's cost kernel under the reference's
+    unmodified lbfgs, driven as pack_dynamics drives it; R
+    (reference_gpu_stack): the reference's own cost kernels, built from its
+    source, under the same lbfgs.  R runs on a smaller batch (its area kernel
+    takes about 100 ms per evaluation of 4096 packings)."""
+    import torch
+
+    from packing_b200.cost import compound_cost
+    lbfgs_ref = reference_lbfgs()
+    if lbfgs_ref is None:
+        why = "reference package not installed in baseline/_ref (python baseline/install_ref.py)"
+        return {"unavailable": why}, {"unavailable": why}
+    n, iters, hist = args.n, args.iters, args.history
+
+    def ours(x, hh, c, g, gh):
+        compound_cost(x, hh, spec, out_cost=c, out_grad=g, out_grad_h=gh)
+
+    Ep = args.plain_E
+    dt, _, cost = time_plain(torch, dev, lbfgs_ref, ours, xyt[:Ep], h[:Ep], iters, hist)
+    p = {"value": Ep / dt, "unit": "relaxations/s", "E": Ep, "seconds": dt,
+         "what": "reference lbfgs (baseline/_ref core/lbfgs_torch_parallel.py, unmodified) driven as "
+                 "pack_dynamics.OptimizerBFGS does, over packing_b200.cost.compound_cost",
+         "mean_final_loss": float(cost.double().mean()), "fused_mean_final_loss": fused_loss,
+         "fused_over_plain_ref": fused_value / (Ep / dt)}
+    r = {"unavailable": "reference kernels not built in oracle/_ref (oracle/build_ref.py)"}
+    try:
+        from oracle import ref_kernels as RK
+        if RK.available():
+            def reference_kernels(x, hh, c, g, gh):
+                cb, gb, _ = RK.boundary(x, hh)
+                co, go = RK.overlap(x, False)
+                torch.add(cb, co, out=c)
+                torch.add(gb, go, out=g)
+                gh.zero_()      # use_fixed_h zeroes every term's h gradient (pack_cost.py:178-189)
+
+            Er = args.refgpu_E
+            dr, _, _ = time_plain(torch, dev, lbfgs_ref, reference_kernels, xyt[:Er], h[:Er], iters, hist)
+            r = {"value": Er / dr, "unit": "relaxations/s", "E": Er, "seconds": dr,
+                 "what": "reference lbfgs (unmodified) over the reference's own CUDA kernels "
+                         "(multi_overlap_list_total area variant + multi_boundary_distance_list_total, "
+                         "pack_cuda.py:482-757) compiled from its source for sm_100a, same GPU",
+                 "fused_over_reference_stack": fused_value / (Er / dr)}
+    except Exception as exc:   # reported; the headline stands
+        r = {"error": f"{type(exc).__name__}: {exc}"}
+    return p, r
+
+
+def measure_c1(args, dev):
+    """64 packings of n = 20 (seed 0), overlap-area cost and
+    its gradient.  CPU: the FP64 oracle on the host's cores (OpenMP over
+    packings), repeated for about 2 s.  GPU: pack_cuda.overlap_multi_ensemble on
+    the same FP32 inputs, CUDA-event timed; its error against FP64."""
+    import torch
+
+    from oracle import oracle as O
+    from packing_b200 import pack_cuda
+    E, n = 64, 20
+    xyt, _ = workload(E, n, seed=0)
+    x64 = xyt.astype(np.float64)
+    O.pair_cost(x64, False)
+    reps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < 2.0:
+        oc, og = O.pair_cost(x64, False)
+        reps += 1
+    cpu_s = (time.perf_counter() - t0) / reps
+    xt = torch.from_numpy(xyt).to(dev)
+    c = torch.empty(E, device=dev)
+    g = torch.empty_like(xt)
+    for _ in range(10):
+        pack_cuda.overlap_multi_ensemble(xt, xt, False, out_cost=c, out_grads=g)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = 200
+    e0.record()
+    for _ in range(k):
+        pack_cuda.overlap_multi_ensemble(xt, xt, False, out_cost=c, out_grads=g)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    gpu_s = e0.elapsed_time(e1) / 1e3 / k
+    cg, gg = c.double().cpu().numpy(), g.double().cpu().numpy()
+    rel = np.abs(cg - oc) / np.maximum(np.abs(oc), 1e-12)
+    return {"workload": f"{E} packings x n={n}, seed 0, overlap-area cost + gradient",
+            "cpu_evals_per_s": E / cpu_s, "cpu_cores": O.num_threads(), "cpu_kind": "port",
+            "cpu_what": "FP64 C restatement of multi_overlap_list_total (area), OpenMP over packings",
+            "gpu_evals_per_s": E / gpu_s, "gpu_us_per_call": gpu_s * 1e6,
+            "gpu_what": "pack_cuda.overlap_multi_ensemble (pk_overlap), one launch per call, CUDA events",
+            "max_cost_rel_err_vs_fp64": float(rel.max()), "max_grad_abs_err_vs_fp64": float(np.abs(gg - og).max()),
+            "tolerances": "cost rtol 1e-5, gradient rtol = atol = 1e-4 (pack_test.py:286-297)"}
+
+
 def run_ours(args, rank, world, dev):
     import torch
 
@@ -374,6 +527,23 @@ def run_ours(args, rank, world, dev):
                                "what": "packing_b200.lbfgs_torch_parallel.lbfgs (per-iteration launches, "
                                        "host loop) over packing_b200.cost.compound_cost",
                                "fused_over_plain": value / (Ep / pt)}
+
+    # ---- the north star's plain forms: the reference's own lbfgs over this
+    # package's cost kernel (P) and over the reference's kernels (R) ----
+    if not args.skip_ref_legs:
+        relax_into(xyt, h, xo, ho, loss, work, spec, prm)
+        torch.cuda.synchronize(dev)
+        p, r = measure_plain_reference(args, dev, xyt, h, spec, value, float(loss.double().mean()))
+        out["plain_reference_lbfgs"] = p
+        out["reference_gpu_stack"] = r
+        if "value" in p:
+            out["fused_over_plain_ref"] = value / p["value"]
+            out["north_star_10x"] = {"target": 10.0, "fused_over_plain_ref": value / p["value"],
+                                     "met": value / p["value"] >= 10.0}
+        try:
+            out["c1"] = measure_c1(args, dev)
+        except Exception as exc:   # reported, the headline stands
+            out["c1"] = {"error": f"{type(exc).__name__}: {exc}"}
 
     # ---- secondary configurations: serving, ragged LUT, GA generation ----
     if not args.skip_extra:
@@ -1013,7 +1183,11 @@ def main():
     ap.add_argument("--plain-E", dest="plain_E", type=int, default=4096)
     ap.add_argument("--cpu-E", dest="cpu_E", type=int, default=128)
     ap.add_argument("--ref-E", dest="ref_E", type=int, default=64)
+    ap.add_argument("--refgpu-E", dest="refgpu_E", type=int, default=1024,
+                    help="packings of the reference-kernel stack leg (R)")
     ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-ref-legs", dest="skip_ref_legs", action="store_true",
+                    help="skip the reference-lbfgs plain forms (P, R) and the C1 block")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-extra", action="store_true", help="skip serving / ragged LUT / GA step")
     ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=10000)

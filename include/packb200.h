@@ -343,7 +343,12 @@ int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* pool, int n_ma
  *     n = 200, history = 10); larger batches return PK_ERANGE with a message.
  *   - The first call on each device looks up the array's device address
  *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *     before any stream capture.  Like every entry point it needs pk_init on
+ *     the device first (PK_ENOTINIT otherwise, before any CUDA call).
+ *   - The address is remembered per device until pk_init runs there again.
+ *     After cudaDeviceReset (or any re-creation of the primary context) call
+ *     pk_init again, as the geometry tables need anyway; the next call then
+ *     fetches the address afresh -- again before any stream capture.
  *   - All calls share the one array and it keeps the previous call's
  *     contents.  Nothing in it needs clearing (every history slot is written
  *     before it is read), but two calls whose kernels overlap on the GPU --

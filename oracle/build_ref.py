@@ -13,7 +13,7 @@ pack_cuda_lut.py:713-726) and runs nvcc with the reference's flags
 (pack_cuda.py:938-945) for sm_100a.  The extracted sources are written to a
 temporary directory only; oracle/_ref/ receives the cubins.
 
-    python oracle/build_ref.py /path/to/reference
+    python oracle/build_ref.py [/path/to/reference]   (default: oracle.refsrc)
 """
 from __future__ import annotations
 
@@ -90,4 +90,6 @@ def build(ref_root):
 
 
 if __name__ == "__main__":
-    print(build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    sys.path.insert(0, os.path.dirname(HERE))
+    from oracle.refsrc import reference_dir
+    print(build(sys.argv[1] if len(sys.argv) > 1 else reference_dir()))

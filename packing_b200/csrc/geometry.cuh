@@ -6,6 +6,11 @@
 
 static thread_local char g_pk_err[512] = "";
 static bool g_pk_inited[64];
+// pk_init calls per device: a cached device address (pk_relax_noalloc's
+// built-in array) taken under an older value is fetched again, so a context
+// re-created after cudaDeviceReset and a fresh pk_init is never served a stale
+// address.
+static unsigned g_pk_init_gen[64];
 
 static int pk_fail(int code, const char* fmt, const char* detail = "")
 {
@@ -215,7 +220,10 @@ extern "C" int pk_init(const PkGeometry* geom_in)
     int dev = 0;
     rc = pk_cuda_check(cudaGetDevice(&dev), "pk_init: cudaGetDevice");
     if (rc) return rc;
-    if (dev >= 0 && dev < 64) g_pk_inited[dev] = true;
+    if (dev >= 0 && dev < 64) {
+        g_pk_inited[dev] = true;
+        ++g_pk_init_gen[dev];
+    }
     return PK_OK;
 }
 

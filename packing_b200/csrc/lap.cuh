@@ -420,10 +420,33 @@ pk_diversity_lap_kernel(const float* __restrict__ pop, const float* __restrict__
     }
 }
 
+// Shared argument checks of the diversity entry points: sizes, the (pop, ref)
+// pair count of a one-CTA-per-pair grid (computed in 64 bits), and the
+// pointers of a launch that has work.
+static int pk_diversity_args(const char* who, const float* pop, const float* ref, int Np, int Nr, int n,
+                             const float* out)
+{
+    if (Np < 0 || Nr < 0 || n < 0) {
+        snprintf(g_pk_err, sizeof(g_pk_err), "%s: negative size", who);
+        return PK_EINVAL;
+    }
+    if ((long long)Np * (long long)Nr > 0x7fffffffLL) {
+        snprintf(g_pk_err, sizeof(g_pk_err), "%s: Np * Nr = %lld pairs exceeds the grid limit 2^31 - 1", who,
+                 (long long)Np * (long long)Nr);
+        return PK_ERANGE;
+    }
+    if ((long long)Np * Nr > 0 && (!out || (n > 0 && (!pop || !ref)))) {
+        snprintf(g_pk_err, sizeof(g_pk_err), "%s: NULL pointer", who);
+        return PK_EINVAL;
+    }
+    return PK_OK;
+}
+
 extern "C" int pk_diversity_costs(const float* pop, const float* ref, int Np, int Nr, int n, int transform,
                                   float* out, void* stream)
 {
-    if (Np < 0 || Nr < 0 || n < 0) return pk_fail(PK_EINVAL, "pk_diversity_costs: negative size%s");
+    int rc = pk_diversity_args("pk_diversity_costs", pop, ref, Np, Nr, n, out);
+    if (rc) return rc;
     const int ntf = transform ? 8 : 1;
     const size_t total = (size_t)ntf * Np * Nr * n * n;
     if (total == 0) return PK_OK;
@@ -435,10 +458,11 @@ extern "C" int pk_diversity_costs(const float* pop, const float* ref, int Np, in
 extern "C" int pk_diversity_matrix(const float* pop, const float* ref, int Np, int Nr, int n, int transform,
                                    float* out, void* stream)
 {
-    if (Np < 0 || Nr < 0 || n < 0) return pk_fail(PK_EINVAL, "pk_diversity_matrix: negative size%s");
+    int rc = pk_diversity_args("pk_diversity_matrix", pop, ref, Np, Nr, n, out);
+    if (rc) return rc;
     if (n > PK_MAX_LAP_N) return pk_fail(PK_ERANGE, "pk_diversity_matrix: more than 256 trees%s");
     if (Np == 0 || Nr == 0) return PK_OK;
-    if (n == 0) return pk_cuda_check(cudaMemsetAsync(out, 0, sizeof(float) * Np * Nr, (cudaStream_t)stream),
+    if (n == 0) return pk_cuda_check(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)Np * Nr, (cudaStream_t)stream),
                                      "pk_diversity_matrix memset");
     const int ntf = transform ? 8 : 1;
     const int cpl = (n + 31) / 32;
@@ -515,9 +539,11 @@ __global__ void pk_diversity_shortcut_kernel(const float* __restrict__ pop, cons
 extern "C" int pk_diversity_shortcut(const float* pop, const float* ref, int Np, int Nr, int n, float cos_a,
                                      float sin_a, int mirror, float* out, void* stream)
 {
-    if (Np < 0 || Nr < 0 || n < 0) return pk_fail(PK_EINVAL, "pk_diversity_shortcut: negative size%s");
+    int rc = pk_diversity_args("pk_diversity_shortcut", pop, ref, Np, Nr, n, out);
+    if (rc) return rc;
+    if (n > 3072) return pk_fail(PK_ERANGE, "pk_diversity_shortcut: more than 3072 trees (48 KB of shared memory)%s");
     if (Np == 0 || Nr == 0) return PK_OK;
-    if (n == 0) return pk_cuda_check(cudaMemsetAsync(out, 0, sizeof(float) * Np * Nr, (cudaStream_t)stream),
+    if (n == 0) return pk_cuda_check(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)Np * Nr, (cudaStream_t)stream),
                                      "pk_diversity_shortcut memset");
     const int T = n < 32 ? 32 : (n > 256 ? 256 : ((n + 31) / 32) * 32);
     pk_diversity_shortcut_kernel<<<Np * Nr, T, (size_t)4 * n * 4, (cudaStream_t)stream>>>(pop, ref, Np, Nr, n, cos_a,

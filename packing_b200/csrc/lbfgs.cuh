@@ -915,12 +915,17 @@ extern "C" int pk_relax_jobs(PkJob* jobs, const int* list, int njobs, float* poo
 
 static __device__ __align__(256) float pk_noalloc_history[PK_NOALLOC_HISTORY_FLOATS];
 static float* g_pk_noalloc_ptr[64];
+static unsigned g_pk_noalloc_gen[64];   // g_pk_init_gen when the address was fetched
 static std::mutex g_pk_noalloc_mu;
 
 extern "C" int pk_relax_noalloc(const float* xyt_in, const float* h_in, int E, int n, const PkCostSpec* spec,
                                 const PkRelaxParams* params, float* xyt_out, float* h_out, float* loss_out,
                                 int* iters_out, void* stream)
 {
+    // the geometry must be on this device before anything touches it (and a
+    // call before pk_init must not create or query a context)
+    int rc = pk_check_init();
+    if (rc) return rc;
     if (!params) return pk_fail(PK_EINVAL, "pk_relax_noalloc: params is NULL%s");
     if (E < 0 || n < 0) return pk_fail(PK_EINVAL, "pk_relax_noalloc: negative size%s");
     if (params->history < 1 || params->history > 64)
@@ -935,18 +940,19 @@ extern "C" int pk_relax_noalloc(const float* xyt_in, const float* h_in, int E, i
         return PK_ERANGE;
     }
     int dev = 0;
-    int rc = pk_cuda_check(cudaGetDevice(&dev), "pk_relax_noalloc: cudaGetDevice");
+    rc = pk_cuda_check(cudaGetDevice(&dev), "pk_relax_noalloc: cudaGetDevice");
     if (rc) return rc;
     if (dev < 0 || dev >= 64) return pk_fail(PK_ERANGE, "pk_relax_noalloc: device id beyond 63%s");
     float* hist = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_pk_noalloc_mu);
-        if (!g_pk_noalloc_ptr[dev]) {
+        if (!g_pk_noalloc_ptr[dev] || g_pk_noalloc_gen[dev] != g_pk_init_gen[dev]) {
             void* p = nullptr;
             rc = pk_cuda_check(cudaGetSymbolAddress(&p, pk_noalloc_history),
                                "pk_relax_noalloc: cudaGetSymbolAddress");
             if (rc) return rc;
             g_pk_noalloc_ptr[dev] = (float*)p;
+            g_pk_noalloc_gen[dev] = g_pk_init_gen[dev];
         }
         hist = g_pk_noalloc_ptr[dev];
     }

@@ -67,6 +67,37 @@ def workspace_floats(sizes, history: int) -> int:
     return 2 * int(history) * sum(3 * int(s) + 3 for s in sizes)
 
 
+def _check_buffers(x, E, h, xyt_out, h_out, loss_out, iters_out, work, history):
+    """The kernel writes through raw pointers: every caller buffer must be a
+    contiguous CUDA array of the right type and at least the size the launch
+    writes, or the launch is refused.  x is (E, n, 3) or ragged (sum n, 3), so
+    x.numel() / 3 trees in either case."""
+    trees = x.numel() // 3
+
+    def need(t, name, dtype, numel, exact=False):
+        if t is None:
+            raise ValueError(f"{name} is required")
+        t = _lib.as_tensor(t, name)
+        if not t.is_cuda or t.device != x.device:
+            raise ValueError(f"{name} must be on {x.device}")
+        if t.dtype != dtype:
+            raise ValueError(f"{name} must have dtype {dtype}, got {t.dtype}")
+        if not t.is_contiguous():
+            raise ValueError(f"{name} must be C-contiguous")
+        if t.numel() < numel or (exact and t.numel() != numel):
+            raise ValueError(f"{name} holds {t.numel()} elements; the launch writes {numel}")
+
+    need(xyt_out, "xyt_out", torch.float32, x.numel(), exact=True)
+    need(loss_out, "loss_out", torch.float32, E)
+    need(work, "work", torch.float32, 2 * int(history) * (3 * trees + 3 * E))
+    if h is not None:
+        need(h, "h", torch.float32, 3 * E)
+    if h_out is not None:
+        need(h_out, "h_out", torch.float32, 3 * E)
+    if iters_out is not None:
+        need(iters_out, "iters_out", torch.int32, E)
+
+
 def relax_into(xyt, h, xyt_out, h_out, loss_out, work, spec: CostSpec, params: RelaxParams, offsets=None,
                order=None, n_max=None, iters_out=None, stream=None, classes=None):
     """Launch the fused relaxation on caller-provided buffers (no host sync,
@@ -82,10 +113,17 @@ def relax_into(xyt, h, xyt_out, h_out, loss_out, work, spec: CostSpec, params: R
     x = _lib.as_tensor(xyt, "xyt")
     _lib.check_f32(x, "xyt")
     if offsets is None:
+        if x.ndim != 3 or x.shape[2] != 3:
+            raise ValueError(f"xyt must be shape (E, n, 3), got {tuple(x.shape)}")
         E, nm = int(x.shape[0]), int(x.shape[1])
     else:
+        if x.ndim != 2 or x.shape[1] != 3:
+            raise ValueError(f"ragged xyt must be shape (sum n, 3), got {tuple(x.shape)}")
+        if n_max is None:
+            raise ValueError("a ragged batch needs n_max")
         E = int(offsets.shape[0]) - 1
         nm = int(n_max)
+    _check_buffers(x, E, h, xyt_out, h_out, loss_out, iters_out, work, params.history_size)
     dev = x.device
     cs = spec.to_c()
     L = _lib.load()

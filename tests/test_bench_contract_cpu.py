@@ -36,3 +36,39 @@ def test_reference_arm_other_ranks_exit_quietly():
                          capture_output=True, text=True, timeout=300, env=env, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     assert not [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_plain_reference_driver_matches_oracle_lbfgs():
+    """bench.py's plain form P runs the reference's own lbfgs (installed
+    unmodified in baseline/_ref) through run_simulation_plain, the flow of
+    pack_dynamics.OptimizerBFGS.run_simulation.  Driven by the FP64 oracle
+    cost on CPU it must reproduce the oracle's lbfgs restatement: the
+    flattening, the objective's buffers and the arguments are right."""
+    import numpy as np
+    import pytest
+    import torch
+    sys.path.insert(0, ROOT)
+    import bench
+    from oracle import oracle as O
+    lbfgs_ref = bench.reference_lbfgs()
+    if lbfgs_ref is None:
+        pytest.skip("reference package not installed (baseline/install_ref.py)")
+    E, n, iters, hist = 3, 10, 30, 5
+    xyt, h = bench.workload(E, n, seed=4)
+
+    def cost_fn(x, hh, c, g, gh):
+        cc, gg, ghh = O.compound_cost(x.numpy(), hh.numpy(), w_area=1e-2, fixed_h=True)
+        c.copy_(torch.from_numpy(cc))
+        g.copy_(torch.from_numpy(gg))
+        gh.copy_(torch.from_numpy(ghh))
+
+    x, _ = bench.run_simulation_plain(lbfgs_ref, cost_fn, torch.from_numpy(xyt).double(),
+                                      torch.from_numpy(h).double(), iters, hist)
+    x0 = np.concatenate([xyt.reshape(E, -1), h], 1).astype(np.float64)
+
+    def f(xx):
+        c, g, gh = O.compound_cost(xx[:, :3 * n].reshape(E, n, 3), xx[:, 3 * n:], w_area=1e-2, fixed_h=True)
+        return c, np.concatenate([g.reshape(E, -1), gh], 1)
+
+    xo, _ = O.lbfgs(f, x0, max_iter=iters, history_size=hist, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+    np.testing.assert_allclose(x.numpy(), xo, rtol=0, atol=1e-10)

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from oracle.refsrc import reference_core
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -102,7 +103,7 @@ def test_oracle_lbfgs_matches_reference_fixture():
     np.testing.assert_allclose(x, d["x_pack"], rtol=0, atol=1e-10)
 
 
-REF = "/root/reference/core"
+REF = reference_core()
 
 
 @pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
