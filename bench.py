@@ -533,7 +533,10 @@ def run_ours(args, rank, world, dev):
     if not args.skip_ref_legs:
         relax_into(xyt, h, xo, ho, loss, work, spec, prm)
         torch.cuda.synchronize(dev)
-        p, r = measure_plain_reference(args, dev, xyt, h, spec, value, float(loss.double().mean()))
+        try:
+            p, r = measure_plain_reference(args, dev, xyt, h, spec, value, float(loss.double().mean()))
+        except Exception as exc:   # reported, the headline stands
+            p = r = {"error": f"{type(exc).__name__}: {exc}"}
         out["plain_reference_lbfgs"] = p
         out["reference_gpu_stack"] = r
         if "value" in p:
