@@ -22,7 +22,8 @@ struct PkCostSmem {
     float4* pose;       // [n_max] x, y, cos, sin
     float* theta;       // [n_max]
     float4* aabb;       // [4*n_max] per piece: minx, maxx, miny, maxy (centre-relative)
-    long long* acc;     // [3*n_max] fixed-point gradient
+    unsigned* acc_lo;   // [3*n_max] fixed-point gradient, low words
+    unsigned* acc_hi;   // [3*n_max] fixed-point gradient, high words
     float4* bnd;        // [n_max] boundary: cost, dh0, dh1, dh2 (unweighted)
     uint32_t* items;    // [cap_items] piece pairs: i | j << 11 | pi << 22 | pj << 24
     uint32_t* near;     // [cap_near] centre-culled pairs: i | j << 11
@@ -30,6 +31,7 @@ struct PkCostSmem {
     double* red;        // [32]
     long long* redl;    // [32]
     float2* piece;      // [16]
+    float4* piece4;     // [8] per piece: (x0, x1, x2, x3), (y0, y1, y2, y3)
     int* piece_nv;      // [4]
     unsigned int* cnt;  // [4] candidate pairs tested, near pairs, piece pairs, evaluations
     int* cell_start;    // [grid_cap + 1] first sorted slot of each grid cell
@@ -38,7 +40,7 @@ struct PkCostSmem {
     int* tcell;         // [n_max] cell of each tree
     int* near_cnt;      // [n_max] near pairs of each sorted position
     int* near_start;    // [n_max + 1] their offsets (exclusive scan)
-    int cap_items, cap_near, grid_cap;
+    int cap_items, cap_near, grid_cap, n_cap;
 };
 
 // Cells of the broad-phase grid (each at least the interaction distance
@@ -67,7 +69,7 @@ __host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap_near, in
     b += (size_t)cap_items * 4;     // items
     b += (size_t)cap_near * 4;      // near pairs
     b += (size_t)(2 * pk_grid_cap(n_max) + 1) * 4 + (size_t)n_max * 16 + 4;   // grid
-    b += 32 * 8 + 32 * 8 + 16 * 8 + 4 * 4 + 16 + 16 + 16 + 16;
+    b += 32 * 8 + 32 * 8 + 16 * 8 + 4 * 4 + 16 + 16 + 16 + 16 + 128;
     return (b + 15) & ~(size_t)15;   // whatever follows starts 16-byte aligned
 }
 
@@ -78,10 +80,12 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
     s.pose = (float4*)p; p += (size_t)n_max * 16;
     s.bnd = (float4*)p; p += (size_t)n_max * 16;
     s.aabb = (float4*)p; p += (size_t)n_max * 64;
+    s.piece4 = (float4*)p; p += 8 * 16;   // 16-byte aligned: every offset so far is a multiple of 16
     // 8-byte arrays next: every offset up to here is a multiple of 16
     s.red = (double*)p; p += 32 * 8;
     s.redl = (long long*)p; p += 32 * 8;
-    s.acc = (long long*)p; p += (size_t)n_max * 24;
+    s.acc_lo = (unsigned*)p; p += (size_t)n_max * 12;
+    s.acc_hi = (unsigned*)p; p += (size_t)n_max * 12;
     s.piece = (float2*)p; p += 16 * 8;
     s.theta = (float*)p; p += (size_t)n_max * 4;
     s.items = (uint32_t*)p; p += (size_t)cap_items * 4;
@@ -99,6 +103,7 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
     p += 16;
     s.cap_items = cap_items;
     s.cap_near = cap_near;
+    s.n_cap = n_max;
     return s;
 }
 
@@ -139,6 +144,43 @@ __device__ __forceinline__ void pk_side_values(const float2 (&X)[4], const float
     for (int k = 0; k < 4; ++k)
 #pragma unroll
         for (int v = 0; v < 4; ++v) f[k][v] = pk_cross3_rn(Y[k], Y[(k + 1) & 3], X[v]);
+}
+
+// A convex piece's four vertices packed in pairs for the FP32x2 instructions
+// of sm_100 (FFMA2 / FMUL2: two independent FP32 operations, each rounded
+// like its scalar form): x01 = (x0, x1), x23 = (x2, x3), likewise y.
+struct PkQuad { float2 x01, x23, y01, y23; };
+
+__device__ __forceinline__ float2 pk_qv(const PkQuad& q, int v)
+{
+    return v == 0 ? make_float2(q.x01.x, q.y01.x) : v == 1 ? make_float2(q.x01.y, q.y01.y)
+         : v == 2 ? make_float2(q.x23.x, q.y23.x) : make_float2(q.x23.y, q.y23.y);
+}
+
+__device__ __forceinline__ PkQuad pk_quad(const float2 (&V)[4])
+{
+    PkQuad q;
+    q.x01 = make_float2(V[0].x, V[1].x); q.x23 = make_float2(V[2].x, V[3].x);
+    q.y01 = make_float2(V[0].y, V[1].y); q.y23 = make_float2(V[2].y, V[3].y);
+    return q;
+}
+
+// f[k][v] for the four lines of Y, two vertices of X per instruction, with
+// the rounding of pk_cross3_rn (the vertex is taken relative to the line's
+// first point before the cross product, which keeps small side values
+// accurate wherever the pieces lie).
+__device__ __forceinline__ void pk_side_values_q(const PkQuad& X, const PkQuad& Y, float (&f)[4][4])
+{
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 a = pk_qv(Y, k), b = pk_qv(Y, (k + 1) & 3);
+        const float ex = b.x - a.x, ey = b.y - a.y;
+        const float2 ex2 = make_float2(ex, ex), ney2 = make_float2(-ey, -ey);
+        const float2 nax2 = make_float2(-a.x, -a.x), nay2 = make_float2(-a.y, -a.y);   // x - a = x + (-a), exactly
+        const float2 f01 = __ffma2_rn(ex2, __fadd2_rn(X.y01, nay2), __fmul2_rn(ney2, __fadd2_rn(X.x01, nax2)));
+        const float2 f23 = __ffma2_rn(ex2, __fadd2_rn(X.y23, nay2), __fmul2_rn(ney2, __fadd2_rn(X.x23, nax2)));
+        f[k][0] = f01.x; f[k][1] = f01.y; f[k][2] = f23.x; f[k][3] = f23.y;
+    }
 }
 
 // One pass of the assembly: the portions of X's edges inside Y, added to A2
@@ -235,18 +277,19 @@ __device__ __forceinline__ bool pk_clip_pass(const float2 (&X)[4], bool x_tri, c
     return true;
 }
 
-__device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_tri,
-                                                   const float2 (&Q)[4], bool q_tri, float2 d,
-                                                   float& area, float3& gP, float3& gQ)
+__device__ __forceinline__ void pk_piece_area_grad_q(const PkQuad& PQ, bool p_tri, const PkQuad& QQ, bool q_tri,
+                                                     float2 d, float& area, float3& gP, float3& gQ)
 {
     float A2 = 0.f;   // twice the area
     gP = make_float3(0.f, 0.f, 0.f);
     gQ = make_float3(0.f, 0.f, 0.f);
     area = 0.f;
+    const float2 P[4] = {pk_qv(PQ, 0), pk_qv(PQ, 1), pk_qv(PQ, 2), pk_qv(PQ, 3)};
+    const float2 Q[4] = {pk_qv(QQ, 0), pk_qv(QQ, 1), pk_qv(QQ, 2), pk_qv(QQ, 3)};
     float f[4][4];
-    pk_side_values(P, Q, f);
+    pk_side_values_q(PQ, QQ, f);
     if (!pk_clip_pass<false>(P, p_tri, Q, q_tri, f, make_float2(0.f, 0.f), A2, gP)) return;
-    pk_side_values(Q, P, f);
+    pk_side_values_q(QQ, PQ, f);
     if (!pk_clip_pass<true>(Q, q_tri, P, p_tri, f, d, A2, gQ)) {
         gP = make_float3(0.f, 0.f, 0.f);
         return;
@@ -257,6 +300,13 @@ __device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_
         gP = make_float3(0.f, 0.f, 0.f);
         gQ = make_float3(0.f, 0.f, 0.f);
     }
+}
+
+__device__ __forceinline__ void pk_piece_area_grad(const float2 (&P)[4], bool p_tri,
+                                                   const float2 (&Q)[4], bool q_tri, float2 d,
+                                                   float& area, float3& gP, float3& gQ)
+{
+    pk_piece_area_grad_q(pk_quad(P), p_tri, pk_quad(Q), q_tri, d, area, gP, gQ);
 }
 
 // ---------------------------------------------------------------------------
@@ -402,6 +452,28 @@ __device__ __forceinline__ void pk_fx_add(long long* a, long long v)
     if (up) atomicAdd(&w[1], up);
 }
 
+// The same add on a split accumulator: low words in one array, high words
+// in another, so consecutive accumulators use consecutive banks.
+__device__ __forceinline__ void pk_fx_add2(unsigned* lo_w, unsigned* hi_w, long long v)
+{
+    const unsigned lo = (unsigned)v, hi = (unsigned)((unsigned long long)v >> 32);
+    const unsigned old = atomicAdd(lo_w, lo);
+    const unsigned up = hi + (unsigned)(old + lo < old);
+    if (up) atomicAdd(hi_w, up);
+}
+
+__device__ __forceinline__ void pk_acc_add2(const PkCostSmem& sm, int t, float3 g)
+{
+    pk_fx_add2(&sm.acc_lo[3 * t + 0], &sm.acc_hi[3 * t + 0], pk_to_fx(g.x));
+    pk_fx_add2(&sm.acc_lo[3 * t + 1], &sm.acc_hi[3 * t + 1], pk_to_fx(g.y));
+    pk_fx_add2(&sm.acc_lo[3 * t + 2], &sm.acc_hi[3 * t + 2], pk_to_fx(g.z));
+}
+
+__device__ __forceinline__ long long pk_acc_get(const PkCostSmem& sm, int k)
+{
+    return (long long)(((unsigned long long)sm.acc_hi[k] << 32) | (unsigned long long)sm.acc_lo[k]);
+}
+
 __device__ __forceinline__ void pk_acc_add(long long* acc, int t, float3 g)
 {
     pk_fx_add(&acc[3 * t + 0], pk_to_fx(g.x));
@@ -417,6 +489,23 @@ __device__ __forceinline__ void pk_load_piece(const PkCostSmem& sm, int p, float
         const float2 l = sm.piece[p * 4 + v];
         V[v] = make_float2(c * l.x - s * l.y + ox, s * l.x + c * l.y + oy);
     }
+}
+
+// Piece p of a tree rotated by (c, s) and moved by (ox, oy), from the SoA
+// table: two vertices per instruction.
+__device__ __forceinline__ PkQuad pk_load_quad(const PkCostSmem& sm, int p, float c, float s, float ox, float oy)
+{
+    const float4 X = sm.piece4[2 * p], Y = sm.piece4[2 * p + 1];
+    const float2 c2 = make_float2(c, c), s2 = make_float2(s, s), ns2 = make_float2(-s, -s);
+    const float2 ox2 = make_float2(ox, ox), oy2 = make_float2(oy, oy);
+    const float2 x01 = make_float2(X.x, X.y), x23 = make_float2(X.z, X.w);
+    const float2 y01 = make_float2(Y.x, Y.y), y23 = make_float2(Y.z, Y.w);
+    PkQuad q;
+    q.x01 = __fadd2_rn(__ffma2_rn(c2, x01, __fmul2_rn(ns2, y01)), ox2);
+    q.x23 = __fadd2_rn(__ffma2_rn(c2, x23, __fmul2_rn(ns2, y23)), ox2);
+    q.y01 = __fadd2_rn(__ffma2_rn(s2, x01, __fmul2_rn(c2, y01)), oy2);
+    q.y23 = __fadd2_rn(__ffma2_rn(s2, x23, __fmul2_rn(c2, y23)), oy2);
+    return q;
 }
 
 // Phase B: evaluate every listed item; returns this thread's fixed-point
@@ -459,13 +548,15 @@ __device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, cons
             gj = (r == i) ? go : gr;
         } else {
             const int pi = (it >> 22) & 3, pj = (it >> 24) & 3;
-            float2 P[4], Q[4];
-            pk_load_piece(sm, pi, A.z, A.w, 0.f, 0.f, P);
-            pk_load_piece(sm, pj, B.z, B.w, d.x, d.y, Q);
             const bool pt = sm.piece_nv[pi] == 3, qt = sm.piece_nv[pj] == 3;
             if (MODE == PK_PAIR_AREA) {
-                pk_piece_area_grad(P, pt, Q, qt, d, val, gi, gj);
+                const PkQuad PQ = pk_load_quad(sm, pi, A.z, A.w, 0.f, 0.f);
+                const PkQuad QQ = pk_load_quad(sm, pj, B.z, B.w, d.x, d.y);
+                pk_piece_area_grad_q(PQ, pt, QQ, qt, d, val, gi, gj);
             } else {
+                float2 P[4], Q[4];
+                pk_load_piece(sm, pi, A.z, A.w, 0.f, 0.f, P);
+                pk_load_piece(sm, pj, B.z, B.w, d.x, d.y, Q);
                 float sp;
                 pk_piece_sat_grad(P, pt, Q, qt, d, sp, gi, gj);
                 const float f = 2.0f * sp;
@@ -476,8 +567,8 @@ __device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, cons
         }
         if (val != 0.f || gi.x != 0.f || gi.y != 0.f || gi.z != 0.f) {
             tot += pk_to_fx(w_pair * val);
-            pk_acc_add(sm.acc, i, make_float3(w_pair * gi.x, w_pair * gi.y, w_pair * gi.z));
-            pk_acc_add(sm.acc, j, make_float3(w_pair * gj.x, w_pair * gj.y, w_pair * gj.z));
+            pk_acc_add2(sm, i, make_float3(w_pair * gi.x, w_pair * gi.y, w_pair * gi.z));
+            pk_acc_add2(sm, j, make_float3(w_pair * gj.x, w_pair * gj.y, w_pair * gj.z));
         }
     }
     return tot;
@@ -530,10 +621,10 @@ __device__ __forceinline__ long long pk_flush_near(const PkCostSmem& sm, int cn,
                 const float dx = B.x - A.x, dy = B.y - A.y;
 #pragma unroll
                 for (int p = 0; p < 4; ++p) {
-                    const float4 a = sm.aabb[4 * i + p];
+                    const float4 a = sm.aabb[p * sm.n_cap + i];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const float4 b = sm.aabb[4 * j + q];
+                        const float4 b = sm.aabb[q * sm.n_cap + j];
                         const bool ov = !(a.y < b.x + dx || b.y + dx < a.x || a.w < b.z + dy || b.w + dy < a.z);
                         mask |= (uint32_t)ov << (4 * p + q);
                     }
@@ -634,7 +725,13 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
     float half = 0.f, hox = 0.f, hoy = 0.f;
     if (H) { half = H[0] * 0.5f; hox = H[1]; hoy = H[2]; }
     // piece table into shared memory first: phase 0 reads it
-    if (threadIdx.x < 16) sm.piece[threadIdx.x] = c_geom.piece[threadIdx.x >> 2][threadIdx.x & 3];
+    if (threadIdx.x < 16) {
+        const float2 v = c_geom.piece[threadIdx.x >> 2][threadIdx.x & 3];
+        sm.piece[threadIdx.x] = v;
+        float* soa = (float*)sm.piece4;   // piece p: x at [8p + v], y at [8p + 4 + v]
+        soa[8 * (threadIdx.x >> 2) + (threadIdx.x & 3)] = v.x;
+        soa[8 * (threadIdx.x >> 2) + 4 + (threadIdx.x & 3)] = v.y;
+    }
     if (threadIdx.x < 4) sm.piece_nv[threadIdx.x] = c_geom.piece_nv[threadIdx.x];
     __syncthreads();
     // ---- phase 0: per tree -------------------------------------------------
@@ -659,7 +756,7 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
                     bb.z = fminf(bb.z, V[v].y); bb.w = fmaxf(bb.w, V[v].y);
                 }
                 const float eps = 1e-6f;
-                sm.aabb[4 * t + p] = make_float4(bb.x - eps, bb.y + eps, bb.z - eps, bb.w + eps);
+                sm.aabb[p * sm.n_cap + t] = make_float4(bb.x - eps, bb.y + eps, bb.z - eps, bb.w + eps);
             }
         }
         if (do_bnd) {
@@ -691,9 +788,12 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
             a2 = pk_to_fx(wb * gth);
             bnd = make_float4(best, -(dx + dy), -gvx, -gvy);
         }
-        sm.acc[3 * t] = a0;
-        sm.acc[3 * t + 1] = a1;
-        sm.acc[3 * t + 2] = a2;
+        sm.acc_lo[3 * t] = (unsigned)a0;
+        sm.acc_hi[3 * t] = (unsigned)((unsigned long long)a0 >> 32);
+        sm.acc_lo[3 * t + 1] = (unsigned)a1;
+        sm.acc_hi[3 * t + 1] = (unsigned)((unsigned long long)a1 >> 32);
+        sm.acc_lo[3 * t + 2] = (unsigned)a2;
+        sm.acc_hi[3 * t + 2] = (unsigned)((unsigned long long)a2 >> 32);
         sm.bnd[t] = bnd;
     }
     if (threadIdx.x == 0) {
@@ -808,16 +908,15 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
         // rotations (backprop_phenotype, kaggle_support.py:1366-1393 and
         // :1155-1195), combined exactly in fixed point
         for (int t = threadIdx.x; t < ng; t += T) {
-            const long long* a = sm.acc;
-            long long gx = a[3 * t], gy = a[3 * t + 1], gt = a[3 * t + 2];
+            long long gx = pk_acc_get(sm, 3 * t), gy = pk_acc_get(sm, 3 * t + 1), gt = pk_acc_get(sm, 3 * t + 2);
             if (sym == 2) {
                 const int u = 3 * (t + ng);
-                gx -= a[u]; gy -= a[u + 1]; gt += a[u + 2];
+                gx -= pk_acc_get(sm, u); gy -= pk_acc_get(sm, u + 1); gt += pk_acc_get(sm, u + 2);
             } else if (sym == 4) {
                 const int u1 = 3 * (t + ng), u2 = 3 * (t + 2 * ng), u3 = 3 * (t + 3 * ng);
-                gx = gx + a[u1 + 1] - a[u2] - a[u3 + 1];
-                gy = gy - a[u1] - a[u2 + 1] + a[u3];
-                gt = gt + a[u1 + 2] + a[u2 + 2] + a[u3 + 2];
+                gx = gx + pk_acc_get(sm, u1 + 1) - pk_acc_get(sm, u2) - pk_acc_get(sm, u3 + 1);
+                gy = gy - pk_acc_get(sm, u1) - pk_acc_get(sm, u2 + 1) + pk_acc_get(sm, u3);
+                gt = gt + pk_acc_get(sm, u1 + 2) + pk_acc_get(sm, u2 + 2) + pk_acc_get(sm, u3 + 2);
             }
             G[3 * t] = (float)((double)gx * PK_FX_INV);
             G[3 * t + 1] = (float)((double)gy * PK_FX_INV);
