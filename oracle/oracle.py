@@ -57,6 +57,7 @@ def lib():
         L.oracle_hungarian.argtypes = [P, i, i, P, P, P]
         L.oracle_diversity_shortcut.argtypes = [P, P, i, i, i, ctypes.c_float, ctypes.c_float, i, P]
         L.oracle_validate.argtypes = [P, i, i, P, P]
+        L.oracle_count_ops.argtypes = [P, i, i, P]
         L.oracle_num_threads.restype = i
         L.oracle_init(TREE_EXPANSION)
         _lib = L
@@ -94,6 +95,36 @@ def pair_cost(xyt, use_separation=False, grad=True, counters=False):
     lib().oracle_pair_cost(_p(xyt), E, n, int(bool(use_separation)), _p(cost), _p(g), _p(cnt))
     out = (cost, g)
     return out + (cnt,) if counters else out
+
+
+def count_ops(xyt):
+    """Algorithmic floating-point work of the overlap-area + boundary cost with
+    both gradients, counted on the reference's arithmetic (see
+    oracle_count_ops in pack_oracle.c).  Returns a dict of total operations
+    per part and of the units they are counted over."""
+    xyt = np.ascontiguousarray(xyt, dtype=np.float64)
+    E, n, _ = xyt.shape
+    out = np.zeros(9, dtype=np.int64)
+    lib().oracle_count_ops(_p(xyt), E, n, _p(out))
+    keys = ["ops_tree", "ops_boundary", "ops_cull", "ops_aabb", "ops_narrow", "trees", "pairs", "near_pairs",
+            "piece_pairs"]
+    return dict(zip(keys, (int(v) for v in out)))
+
+
+def lbfgs_ops(N, history_entries):
+    """Floating-point operations of one iteration of the reference's lbfgs
+    without line search (lbfgs_torch_parallel.py:531-724) for one system of N
+    parameters, counted on its tensor expressions (add, sub, mul, div, cmp,
+    |.| = 1; a sum over N elements = N):
+      two-loop, per history entry: s.q sum (2N) and q - y a mask (3N) in the
+        first loop (:548-554); y.r sum (2N), s (al - be) (N) and r + u mask
+        (2N) in the second (:564-572): 10N;
+      per iteration: r = q H (N, :558); the max_step clamp |d t| max (2N,
+        :594); gtd (2N, :603); x + t d (2N, :631); y = g - g_prev, s = d t,
+        y.s, y.y (6N, :639-651); the convergence tests |g| max, d t, |s|
+        max (3N, :694-704): 16N.
+    Terms independent of N (the scalar updates) are left out."""
+    return 10 * N * int(history_entries) + 16 * N
 
 
 def pair_cost_crystal(xyt, crystal_axes, use_separation=False, only_self_interactions=False, n_periodic=2,

@@ -164,15 +164,25 @@ void oracle_geometry(double* piece_xy /*4*4*2*/, int* piece_nv /*4*/,
     radius_cutoff_area[2] = g_tree_area;
 }
 
+/* ---- op counting ---------------------------------------------------------
+ * oracle_count_ops (below) sets g_ops while it runs, single-threaded; the
+ * primitives then add their floating-point operations to it: add, sub, mul,
+ * div, sqrt, comparison and |x| count 1 each, a negation 0 (the C source
+ * holds no fused multiply-add).  Every other caller runs with g_ops NULL. */
+static int64_t* g_ops = NULL;
+#define OPS(k) do { if (g_ops) *g_ops += (k); } while (0)
+
 /* ---- primitives: pack_cuda_primitives.py ------------------------------- */
 
 static double cross3(d2 a, d2 b, d2 c)   /* :20 */
 {
+    OPS(7);   /* 4 sub, 2 mul, 1 sub */
     return (b.x - a.x) * (c.y - a.y) - (b.y - a.y) * (c.x - a.x);
 }
 
 static d2 line_isect(d2 p1, d2 p2, d2 q1, d2 q2)   /* :25-41 */
 {
+    OPS(17);  /* r, s: 4; den: 3; numerator: 5; t: 1; the point: 4 */
     double rx = p2.x - p1.x, ry = p2.y - p1.y;
     double sx = q2.x - q1.x, sy = q2.y - q1.y;
     double den = rx * sy - ry * sx;
@@ -184,6 +194,7 @@ static d2 line_isect(d2 p1, d2 p2, d2 q1, d2 q2)   /* :25-41 */
 static void line_isect_bwd(d2 p1, d2 p2, d2 q1, d2 q2, d2 g,
                            d2* gp1, d2* gp2, d2* gq1, d2* gq2)
 {
+    OPS(94);  /* r, s, den, num, t, den^2: 14; tp1..tq2: 34; gp1..gq2: 46 */
     double rx = p2.x - p1.x, ry = p2.y - p1.y;
     double sx = q2.x - q1.x, sy = q2.y - q1.y;
     double den = rx * sy - ry * sx;
@@ -222,6 +233,7 @@ static int clip_edge(const d2* in, int nin, d2 A, d2 B, d2* out, clipmeta* m)
         d2 E = in[i];
         double es = cross3(A, B, E);
         int sin_ = ss >= 0.0, ein = es >= 0.0;
+        OPS(2);
         if (sin_ && ein) {
             out[k] = E; m->type[k] = 0; m->i1[k] = i; ++k;
         } else if (sin_ && !ein) {
@@ -262,8 +274,10 @@ static double convex_isect_area(const d2* subj, int ns, const d2* clip, int nc, 
     }
     double sa = 0.5 * sum;
     double area = sa >= 0.0 ? sa : -sa;
+    OPS(4 * fn + 2);   /* shoelace: 2 mul, 1 sub, 1 add per vertex; 0.5 *; |.| */
     if (!d_subj || area == 0.0) return area;
     double sg = sa >= 0.0 ? 1.0 : -1.0;
+    OPS(2 + 6 * fn);   /* area == 0, sign; dA/dv per vertex: 2 x (sub, 2 mul) */
     d2 cur[MAXI], nxt[MAXI];
     for (int k = 0; k < fn; ++k) {
         int kp = (k - 1 + fn) % fn, kn = (k + 1) % fn;
@@ -276,7 +290,9 @@ static double convex_isect_area(const d2* subj, int ns, const d2* clip, int nc, 
             if (meta[e].type[i] == 0) {
                 nxt[meta[e].i1[i]].x += cur[i].x;
                 nxt[meta[e].i1[i]].y += cur[i].y;
+                OPS(2);
             } else {
+                OPS(4);
                 d2 gS, gE, gA, gB;
                 int a = meta[e].i1[i], b = meta[e].i2[i];
                 line_isect_bwd(polys[e][a], polys[e][b], A, B, cur[i], &gS, &gE, &gA, &gB);
@@ -830,6 +846,76 @@ void oracle_validate(const double* xyt, int E, int n, int* overlaps, double* sid
         overlaps[e] = cnt;
         side[e] = n > 0 ? fmax(bx1 - bx0, by1 - by0) : 0.0;
     }
+}
+
+/* Algorithmic work of one evaluation of the overlap-area + boundary cost with
+ * both pose gradients, counted on the reference's arithmetic (the functions
+ * above restate pack_cuda_primitives.py:20-538 and pack_cuda.py:95-136,
+ * 254-642 operation for operation).  Per packing:
+ *   tree:     sin + cos (2) and the 4 piece transforms with their boxes
+ *             (compute_tree_poly_and_aabb, 12 per vertex), once per tree;
+ *   boundary: boundary_distance_tree per tree (338, counted below);
+ *   cull:     every unordered pair's centre test (2 sub, 2 mul, add, cmp);
+ *   aabb:     16 box tests of 4 comparisons per pair within the cutoff;
+ *   narrow:   per unordered piece pair whose boxes overlap, the reference's
+ *             clip + backward for each piece against the other (the
+ *             reference evaluates both orders) and each piece's pose
+ *             backward (backward_transform_vertices, 12 per vertex) when the
+ *             area is nonzero, plus the two partial sums.
+ * out[0..4]: ops of tree, boundary, cull, aabb, narrow; out[5..8]: trees,
+ * unordered pairs, near pairs, piece pairs.  Single-threaded. */
+void oracle_count_ops(const double* xyt, int E, int n, int64_t* out)
+{
+    int64_t ops[5] = {0, 0, 0, 0, 0}, units[4] = {0, 0, 0, 0};
+    int nv_total = 0;
+    for (int p = 0; p < MAXP; ++p) nv_total += g_piece_nv[p];
+    d2* wp = (d2*)malloc(sizeof(d2) * (size_t)n * MAXP * MAXV);
+    double* bb = (double*)malloc(sizeof(double) * (size_t)n * MAXP * 4);
+    for (int e = 0; e < E; ++e) {
+        const double* X = xyt + (size_t)e * n * 3;
+        for (int i = 0; i < n; ++i) {
+            double c = cos(X[3 * i + 2]), s = sin(X[3 * i + 2]);
+            for (int p = 0; p < MAXP; ++p)
+                piece_world(X[3 * i], X[3 * i + 1], c, s, p, wp + ((size_t)i * MAXP + p) * MAXV,
+                            bb + ((size_t)i * MAXP + p) * 4);
+        }
+        ops[0] += (int64_t)n * (2 + 12 * nv_total);
+        /* boundary_distance_tree: per outline vertex 20 (transform 2 x (2 mul,
+         * 3 add/sub), 2 |.|, 2 x (cmp, sub), dx^2 + dy^2, cmp); then 38 for
+         * the sum, the winning vertex again (16) and the gradients (21) */
+        ops[1] += (int64_t)n * (NTV * 20 + 38);
+        units[0] += n;
+        for (int i = 0; i < n; ++i)
+            for (int j = i + 1; j < n; ++j) {
+                double dx = X[3 * j] - X[3 * i], dy = X[3 * j + 1] - X[3 * i + 1];
+                ops[2] += 6;
+                ++units[1];
+                if (dx * dx + dy * dy > g_cutoff_sq) continue;
+                ++units[2];
+                ops[3] += 16 * 4;
+                for (int pi = 0; pi < MAXP; ++pi)
+                    for (int pj = 0; pj < MAXP; ++pj) {
+                        const double* rb = bb + ((size_t)i * MAXP + pi) * 4;
+                        const double* ob = bb + ((size_t)j * MAXP + pj) * 4;
+                        if (rb[1] < ob[0] || ob[1] < rb[0] || rb[3] < ob[2] || ob[3] < rb[2]) continue;
+                        ++units[3];
+                        const d2* P = wp + ((size_t)i * MAXP + pi) * MAXV;
+                        const d2* Q = wp + ((size_t)j * MAXP + pj) * MAXV;
+                        d2 dsub[MAXV];
+                        g_ops = &ops[4];
+                        double a1 = convex_isect_area(P, g_piece_nv[pi], Q, g_piece_nv[pj], dsub);
+                        double a2 = convex_isect_area(Q, g_piece_nv[pj], P, g_piece_nv[pi], dsub);
+                        g_ops = NULL;
+                        ops[4] += 2;   /* the partial sums */
+                        if (a1 != 0.0) ops[4] += 12 * g_piece_nv[pi];
+                        if (a2 != 0.0) ops[4] += 12 * g_piece_nv[pj];
+                    }
+            }
+    }
+    free(wp);
+    free(bb);
+    for (int k = 0; k < 5; ++k) out[k] = ops[k];
+    for (int k = 0; k < 4; ++k) out[5 + k] = units[k];
 }
 
 int oracle_num_threads(void)

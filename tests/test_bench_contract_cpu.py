@@ -72,3 +72,23 @@ def test_plain_reference_driver_matches_oracle_lbfgs():
 
     xo, _ = O.lbfgs(f, x0, max_iter=iters, history_size=hist, max_step=0.01, tolerance_grad=0, tolerance_change=0)
     np.testing.assert_allclose(x.numpy(), xo, rtol=0, atol=1e-10)
+
+
+def test_roofline_work_constants_match_oracle_op_counts():
+    """bench.py's algorithmic work per unit equals the oracle's op count of
+    the reference arithmetic: cull, box tests, per-tree work, the average
+    piece pair on the seeded 8 x n = 200 initial packings, and the lbfgs
+    iteration (lbfgs_torch_parallel.py:531-724)."""
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import bench
+    from oracle import oracle as O
+    x, _ = bench.workload(8, 200, seed=0)
+    d = O.count_ops(x.astype(np.float64))
+    assert d["pairs"] == 8 * 200 * 199 // 2 and d["trees"] == 1600
+    assert d["ops_cull"] == bench.FLOPS_PER_PAIR * d["pairs"]
+    assert d["ops_aabb"] == bench.FLOPS_PER_NEAR * d["near_pairs"]
+    assert d["ops_tree"] + d["ops_boundary"] == bench.FLOPS_PER_TREE * d["trees"]
+    assert round(d["ops_narrow"] / d["piece_pairs"]) == bench.FLOPS_PER_PIECE_PAIR
+    N, m = 603, 10
+    assert O.lbfgs_ops(N, m) == bench.FLOPS_PER_HIST_ELEM * N * m + bench.FLOPS_PER_ITER_ELEM * N
