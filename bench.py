@@ -593,9 +593,11 @@ def _serve_requests(count, seed):
 
 def measure_serve(args, dev):
     """10,000 requests, n log-uniform in [10, 200], 50-300 iterations, Poisson
-    arrivals at ~80% of the measured service capacity; against the same jobs
-    run batch by batch through the plain drop-in (grouped by tree count as
-    pack_dynamics.run_simulation_list does)."""
+    arrivals at ~80% of the measured service capacity (a saturating burst of
+    args.serve_burst requests through the pipelined engine); against the
+    engine's ceiling on the same mix and the same jobs run batch by batch
+    through the plain forms (grouped by tree count and budget, as
+    pack_dynamics.run_simulation_list groups by tree count)."""
     import torch
 
     from packing_b200.cost import CostSpec, compound_cost
@@ -618,36 +620,74 @@ def measure_serve(args, dev):
     stats, done = srv.run_trace(reqs, arrivals)
     # jobs that met the reference's own stop tests before their iteration budget
     stopped_early = sum(1 for r in done if r.iterations < r.iters)
-    # batch-by-batch plain form on a subset: all requests available, batches
-    # of args.serve_plain_batch, one drop-in lbfgs per distinct tree count
-    sub = reqs[:args.serve_plain]
-    t0 = time.perf_counter()
-    for b0 in range(0, len(sub), args.serve_plain_batch):
-        batch = sub[b0:b0 + args.serve_plain_batch]
-        groups = {}
-        for xyt, h, it in batch:
-            groups.setdefault(xyt.shape[0], []).append((xyt, h, it))
-        for n, grp in groups.items():
-            E = len(grp)
-            it = max(g[2] for g in grp)
-            x0 = torch.from_numpy(np.stack([np.concatenate([g[0].reshape(-1), g[1]]) for g in grp])).to(dev)
-            cb = torch.empty(E, device=dev)
-            gb = torch.empty((E, n, 3), device=dev)
-            ghb = torch.empty((E, 3), device=dev)
+    # the engine's ceiling on the same mix: every burst job resident at once,
+    # one step of chunk 300 (so each job runs to its own budget in one launch
+    # per size class), device time of the launches only
+    srv = RelaxServer(spec, history=hist, chunk_iters=300, device=dev)
+    for xyt, h, it in burst[:64]:
+        srv.submit(xyt, h, it)
+    srv.timed_step()
+    srv = RelaxServer(spec, history=hist, chunk_iters=300, device=dev)
+    for xyt, h, it in burst:
+        srv.submit(xyt, h, it)
+    done_c, dev_s = srv.timed_step()
+    if len(done_c) != len(burst):
+        raise RuntimeError("the ceiling step did not finish every burst job")
+    ceiling = len(burst) / dev_s
+    # batch-by-batch plain forms on a subset: all requests available, batches
+    # of args.serve_plain_batch, one relaxation per distinct (tree count,
+    # iteration budget) -- static batching that runs each job to its own
+    # budget.  P: the reference's own lbfgs over this package's cost kernel
+    # (run_simulation_plain); also this package's drop-in lbfgs.
+    def plain_rate(sub, relax_group):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for b0 in range(0, len(sub), args.serve_plain_batch):
+            batch = sub[b0:b0 + args.serve_plain_batch]
+            groups = {}
+            for xyt, h, it in batch:
+                groups.setdefault((xyt.shape[0], it), []).append((xyt, h, it))
+            for (n, it), grp in groups.items():
+                xg = torch.from_numpy(np.stack([g[0] for g in grp])).to(dev)
+                hg = torch.from_numpy(np.stack([g[1] for g in grp])).to(dev)
+                relax_group(xg, hg, it).cpu()
+        return len(sub) / (time.perf_counter() - t0)
 
-            def f(x, is_main, n=n, E=E, cb=cb, gb=gb, ghb=ghb):
-                compound_cost(x[:, :3 * n].reshape(E, n, 3).contiguous(), x[:, 3 * n:].contiguous(), spec,
-                              out_cost=cb, out_grad=gb, out_grad_h=ghb)
-                return cb, torch.cat([gb.reshape(E, -1), ghb], 1)
+    def ours_cost(x, hh, c, g, gh):
+        compound_cost(x, hh, spec, out_cost=c, out_grad=g, out_grad_h=gh)
 
-            lbfgs(f, x0, max_iter=it, history_size=hist, max_step=0.01, tolerance_grad=0, tolerance_change=0)
-            x0.cpu()
-    plain = len(sub) / (time.perf_counter() - t0)
+    def dropin_group(xg, hg, it):
+        E, n = int(xg.shape[0]), int(xg.shape[1])
+        x0 = torch.cat([xg.reshape(E, -1), hg], 1).contiguous()
+        cb, gb, ghb = torch.empty(E, device=dev), torch.empty_like(xg), torch.empty_like(hg)
+
+        def f(x, is_main):
+            compound_cost(x[:, :3 * n].reshape(E, n, 3).contiguous(), x[:, 3 * n:].contiguous(), spec,
+                          out_cost=cb, out_grad=gb, out_grad_h=ghb)
+            return cb, torch.cat([gb.reshape(E, -1), ghb], 1)
+
+        return lbfgs(f, x0, max_iter=it, history_size=hist, max_step=0.01, tolerance_grad=0, tolerance_change=0)
+
+    plain_dropin = plain_rate(reqs[:args.serve_plain], dropin_group)
+    lbfgs_ref = reference_lbfgs()
+    plain_ref = None
+    if lbfgs_ref is not None:
+        plain_ref = plain_rate(reqs[:args.serve_plain_ref],
+                               lambda xg, hg, it: run_simulation_plain(lbfgs_ref, ours_cost, xg, hg, it, hist)[0])
+    plain = plain_ref if plain_ref is not None else plain_dropin
     return {"requests": stats["requests"], "arrival_rate_per_s": rate, "capacity_per_s": capacity,
+            "ceiling_per_s": ceiling, "capacity_over_ceiling": capacity / ceiling,
+            "ceiling_what": f"device time of the same engine's launches with all {len(burst)} burst jobs "
+                            "resident and one chunk of 300 iterations (each job to its own budget)",
             "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"], "relaxations_per_s": stats["relaxations_per_s"],
             "engine_launches": stats["launches"], "chunk_iters": args.serve_chunk,
-            "plain_batch_by_batch_per_s": plain, "plain_sample": f"first {len(sub)} requests, batches of "
-                                                                 f"{args.serve_plain_batch}, grouped by n",
+            "plain_batch_by_batch_per_s": plain,
+            "plain_what": ("P: the reference's lbfgs (baseline/_ref, unmodified) over packing_b200.cost.compound_cost"
+                           if plain_ref is not None else "this package's drop-in lbfgs (reference not installed)"),
+            "plain_sample": f"first {args.serve_plain_ref if plain_ref is not None else args.serve_plain} requests, "
+                            f"batches of {args.serve_plain_batch}, one relaxation per (n, iteration budget)",
+            "plain_dropin_batch_by_batch_per_s": plain_dropin,
+            "plain_dropin_sample": f"first {args.serve_plain} requests, this package's drop-in lbfgs",
             "served_over_plain": stats["relaxations_per_s"] / plain, "jobs_stopped_early": stopped_early,
             "workload": "n log-uniform [10,200], iterations U{50..300}, Poisson arrivals at 0.8 x capacity, m="
                         f"{hist}, max_step 0.01, boundary + overlap area"}
@@ -1211,8 +1251,9 @@ def main():
     ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=10000)
     ap.add_argument("--serve-burst", dest="serve_burst", type=int, default=2000)
     ap.add_argument("--serve-chunk", dest="serve_chunk", type=int, default=25)
-    ap.add_argument("--serve-plain", dest="serve_plain", type=int, default=512)
-    ap.add_argument("--serve-plain-batch", dest="serve_plain_batch", type=int, default=256)
+    ap.add_argument("--serve-plain", dest="serve_plain", type=int, default=128)
+    ap.add_argument("--serve-plain-ref", dest="serve_plain_ref", type=int, default=32)
+    ap.add_argument("--serve-plain-batch", dest="serve_plain_batch", type=int, default=128)
     ap.add_argument("--lut-E", dest="lut_E", type=int, default=8192)
     ap.add_argument("--ga-P", dest="ga_P", type=int, default=2048)
     ap.add_argument("--ga-iters", dest="ga_iters", type=int, default=100)
