@@ -46,11 +46,15 @@ def gather_results(local: torch.Tensor, counts, group=None) -> torch.Tensor:
     rank = dist.get_rank(group)
     k = local.shape[1]
     mx = max(counts) if counts else 0
-    buf = torch.zeros((mx, k), dtype=local.dtype, device=local.device)
-    buf[:counts[rank]] = local
+    # gloo gathers host tensors: a CUDA table goes through host memory there
+    # (NCCL gathers it in place)
+    via_host = local.is_cuda and dist.get_backend(group) == "gloo"
+    dev = torch.device("cpu") if via_host else local.device
+    buf = torch.zeros((mx, k), dtype=local.dtype, device=dev)
+    buf[:counts[rank]] = local.to(dev)
     parts = [torch.empty_like(buf) for _ in range(world)]
     dist.all_gather(parts, buf, group=group)
-    return torch.cat([parts[r][:counts[r]] for r in range(world)], dim=0)
+    return torch.cat([parts[r][:counts[r]] for r in range(world)], dim=0).to(local.device)
 
 
 def relax_shard(xyt_list, h, spec, params, rank: int, world: int, device=None, group=None):
@@ -113,9 +117,11 @@ def gather_champions(xyt: torch.Tensor, fitness: torch.Tensor, offset: int, k: i
     rows[:m, 1] = gidx[pick]
     rows[:m, 2:] = xyt[pick].reshape(m, 3 * n).to(torch.float64)
     if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
-        parts = [torch.empty_like(rows) for _ in range(dist.get_world_size(group))]
-        dist.all_gather(parts, rows, group=group)
-        rows = torch.cat(parts, 0)
+        host = rows.is_cuda and dist.get_backend(group) == "gloo"   # gloo gathers host tensors
+        buf = rows.cpu() if host else rows
+        parts = [torch.empty_like(buf) for _ in range(dist.get_world_size(group))]
+        dist.all_gather(parts, buf, group=group)
+        rows = torch.cat(parts, 0).to(dev)
     rows = rows[rows[:, 1] >= 0]
     sel = best(rows[:, 0], rows[:, 1], min(k, rows.shape[0]))
     out = rows[sel]
