@@ -228,7 +228,8 @@ def compound_cost(xyt, h, w_boundary=1.0, w_overlap=1.0, use_separation=False, w
     cb, gb, ghb = boundary(xyt, h)
     cc, gc = pair_cost(xyt, use_separation)
     h = np.asarray(h, np.float64)
-    cost = w_area * h[:, 0] ** 2 + w_boundary * cb + w_overlap * cc
+    # AreaCost is zero with a fixed side (use_fixed_h, pack_cost.py:1276-1282)
+    cost = (0.0 if fixed_h else w_area) * h[:, 0] ** 2 + w_boundary * cb + w_overlap * cc
     g = w_boundary * gb + w_overlap * gc
     gh = w_boundary * ghb
     gh[:, 0] += w_area * 2.0 * h[:, 0]

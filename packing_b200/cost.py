@@ -2,7 +2,7 @@
 from separate kernels and cupy sums (``core/pack_cost.py:245-277``).
 
 ``compound_cost(xyt, h, ...)`` returns ``(cost (E,), grad (E, n, 3),
-grad_h (E, 3))`` for ``w_area * h0^2 + w_boundary * boundary + w_pair *
+grad_h (E, 3))`` for ``w_area * h0^2 (zero with a fixed side, as AreaCost) + w_boundary * boundary + w_pair *
 pairs``, the form of ``OptimizerBFGS``'s default cost
 (``core/pack_dynamics.py:45-51``: AreaCost 1e-2, BoundaryDistanceCost 1,
 CollisionCostOverlappingArea 1).  Ragged batches go through ``offsets``.

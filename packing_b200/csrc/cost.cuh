@@ -951,7 +951,9 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
         GH[2] = 0.f;
     }
     if (GH && spec.fixed_h && threadIdx.x == 0) { GH[0] = 0.f; GH[1] = 0.f; GH[2] = 0.f; }
-    total += (double)spec.w_area * h0 * h0;
+    // AreaCost is zero with a fixed side, its gradient too (use_fixed_h,
+    // pack_cost.py:1276-1282; every term's h gradient is zeroed, :178-189)
+    if (!spec.fixed_h) total += (double)spec.w_area * h0 * h0;
     __syncthreads();
     return total;
 }

@@ -77,7 +77,19 @@ def test_lut_vs_reference_kernel(cuda, quad):
     pack_cuda_lut.overlap_multi_ensemble(x, c, lut, g)
     torch.cuda.synchronize()
     np.testing.assert_allclose(c.cpu().numpy(), rc.cpu().numpy(), rtol=1e-5, atol=1e-6)
-    np.testing.assert_allclose(g.cpu().numpy(), rg.cpu().numpy(), rtol=1e-3, atol=1e-4)
+    # Gradients: the two FP32 kernels sum a tree's pair terms in different
+    # orders (the reference with float atomics, here exactly in fixed point),
+    # so they are each held to the FP64 evaluation of the same table at the
+    # reference's own gradient tolerance (pack_test.py:286-297), and ours
+    # must be no further from it than the reference kernel is.
+    _, og = O.lut_cost(list(x.cpu().numpy().astype(np.float64)), lut.lut_d.cpu().numpy(), b, quad,
+                       O.geometry()[3])
+    og = np.stack(og)
+    err_ours = np.abs(g.cpu().numpy() - og).max()
+    err_ref = np.abs(rg.cpu().numpy() - og).max()
+    print(f"\nLUT max |grad - FP64|: ours {err_ours:.3g}, reference kernel {err_ref:.3g}")
+    np.testing.assert_allclose(g.cpu().numpy(), og, rtol=1e-4, atol=1e-4)
+    assert err_ours <= err_ref + 1e-6
 
 
 @pytest.mark.parametrize("N", [3, 33, 100, 200])
