@@ -90,6 +90,8 @@ def build(ref_root):
 
 
 if __name__ == "__main__":
-    sys.path.insert(0, os.path.dirname(HERE))
-    from oracle.refsrc import reference_dir
+    # refsrc sits beside this script (imported by file: the package name
+    # "oracle" would resolve to oracle/oracle.py from here)
+    sys.path.insert(0, HERE)
+    from refsrc import reference_dir
     print(build(sys.argv[1] if len(sys.argv) > 1 else reference_dir()))
