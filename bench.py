@@ -187,7 +187,7 @@ FLOPS_PER_ITER_ELEM = 16
 # history); other configurations report null.  Most of it is L-BFGS history
 # (2 m (3n + 3) floats per packing) written back from L2 while packings run;
 # a finished packing's history is discarded from L2, not written back.
-TRAFFIC_BYTES = {(4096, 200, 200, 10): 183.1e6}
+TRAFFIC_BYTES = {(4096, 200, 200, 10): 61.5e6}
 HBM_FALLBACK_GBPS = 6650.0
 
 
