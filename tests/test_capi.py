@@ -63,3 +63,27 @@ def test_probes_reject_bad_arguments_before_launching():
     assert b"pk_gather_probe" in L.pk_last_error()
     assert L.pk_fma_probe(None, 1, 1, 1, None) != 0
     assert b"pk_fma_probe" in L.pk_last_error()
+
+
+def test_diversity_entry_points_check_arguments_on_the_host():
+    """NULL arrays and a (pop, ref) pair count beyond the one-CTA-per-pair
+    grid are refused with a status before any launch (no device needed)."""
+    L = _lib.load()
+    for fn in ("pk_diversity_costs", "pk_diversity_matrix"):
+        assert getattr(L, fn)(None, None, 2, 3, 10, 1, None, None) == -1, fn
+        assert b"NULL" in L.pk_last_error()
+        assert getattr(L, fn)(None, None, 70000, 70000, 10, 1, None, None) == -4, fn
+        assert b"grid limit" in L.pk_last_error()
+    assert L.pk_diversity_shortcut(None, None, 2, 3, 10, 1.0, 0.0, 0, None, None) == -1
+    assert L.pk_diversity_shortcut(None, None, 70000, 70000, 10, 1.0, 0.0, 0, None, None) == -4
+    assert L.pk_diversity_costs(None, None, -1, 3, 10, 1, None, None) == -1
+    assert L.pk_diversity_costs(None, None, 0, 3, 10, 1, None, None) == 0     # nothing to do
+
+
+def test_allocation_free_relaxation_needs_init_first():
+    """pk_relax_noalloc checks pk_init before any CUDA call: on a host where
+    pk_init has not run it returns PK_ENOTINIT."""
+    L = _lib.load()
+    prm = _lib.PkRelaxParams()
+    prm.history = 10
+    assert L.pk_relax_noalloc(None, None, 1, 10, None, ctypes.byref(prm), None, None, None, None, None) != 0

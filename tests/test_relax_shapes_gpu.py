@@ -192,3 +192,31 @@ def test_partial_order_rejects_bad_counts(cuda):
     rc = L.pk_relax_ordered(*args, None, 2, 4, 10, ctypes.byref(cs), ctypes.byref(ps), _lib.ptr(x), None,
                             _lib.ptr(x), None, _lib.ptr(x), None)
     assert rc != 0   # no order
+
+
+def test_relax_into_refuses_short_or_wrong_buffers(cuda):
+    """The kernel writes through raw pointers, so relax_into checks every
+    caller buffer before launching: a history workspace one float short, an
+    output of the wrong size or dtype, or a buffer on the host is a
+    ValueError, and nothing is launched."""
+    from packing_b200.relax import RelaxParams, relax_into, workspace_floats
+    E, n = 4, 30
+    xyt = torch.from_numpy(poses(E, n, seed=3)).to(cuda)
+    h = torch.from_numpy(square_h(E, n)).to(cuda)
+    prm = RelaxParams(n_iterations=5, history_size=4, max_step=0.01)
+    need = workspace_floats([n] * E, 4)
+    ok = dict(xyt_out=torch.empty_like(xyt), h_out=torch.empty_like(h), loss_out=torch.empty(E, device=cuda),
+              work=torch.empty(need, device=cuda))
+    relax_into(xyt, h, ok["xyt_out"], ok["h_out"], ok["loss_out"], ok["work"], _spec(), prm)
+    bad = [dict(ok, work=torch.empty(need - 1, device=cuda)),
+           dict(ok, loss_out=torch.empty(E - 1, device=cuda)),
+           dict(ok, xyt_out=torch.empty((E, n + 1, 3), device=cuda)),
+           dict(ok, xyt_out=torch.empty_like(xyt, dtype=torch.float64)),
+           dict(ok, h_out=torch.empty((E - 1, 3), device=cuda)),
+           dict(ok, work=torch.empty(need))]
+    for b in bad:
+        with pytest.raises(ValueError):
+            relax_into(xyt, h, b["xyt_out"], b["h_out"], b["loss_out"], b["work"], _spec(), prm)
+    with pytest.raises(ValueError):
+        relax_into(xyt, h, ok["xyt_out"], ok["h_out"], ok["loss_out"], ok["work"], _spec(), prm,
+                   iters_out=torch.empty(E, dtype=torch.int64, device=cuda))
