@@ -33,7 +33,9 @@ struct PkCostSmem {
     float2* piece;      // [16]
     float4* piece4;     // [8] per piece: (x0, x1, x2, x3), (y0, y1, y2, y3)
     int* piece_nv;      // [4]
-    unsigned int* cnt;  // [4] candidate pairs tested, near pairs, piece pairs, evaluations
+    unsigned int* cnt;  // [4] candidate pairs tested, near pairs, piece pairs, evaluations; then
+                        // [4] kept near list: state (-1 off, 0 build next, 1 valid), length,
+                        // filter flag, list distance (pk_nlist)
     int* cell_start;    // [grid_cap + 1] first sorted slot of each grid cell
     int* cell_fill;     // [grid_cap] trees per cell, then a scratch cursor
     int* sorted;        // [n_max] tree indices ordered by cell
@@ -58,7 +60,10 @@ __host__ __device__ inline void pk_caps(int T, int mode, int* cap_near, int* cap
     *cap_items = mode == PK_PAIR_LUT ? 0 : 20 * T;
 }
 
-__host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap_near, int cap_items)
+// keep: room for the kept near list's state (the fused relaxation only; a
+// one-shot evaluation keeps the smaller footprint, which lets the smallest
+// size classes fit one more CTA per SM).
+__host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap_near, int cap_items, bool keep = false)
 {
     size_t b = 0;
     b += (size_t)n_max * 16;        // pose
@@ -70,10 +75,12 @@ __host__ __device__ inline size_t pk_cost_smem_bytes(int n_max, int cap_near, in
     b += (size_t)cap_near * 4;      // near pairs
     b += (size_t)(2 * pk_grid_cap(n_max) + 1) * 4 + (size_t)n_max * 16 + 4;   // grid
     b += 32 * 8 + 32 * 8 + 16 * 8 + 4 * 4 + 16 + 16 + 16 + 16 + 128;
+    if (keep) b += 16 + 32 * 4;   // pk_nlist, pk_disp
     return (b + 15) & ~(size_t)15;   // whatever follows starts 16-byte aligned
 }
 
-__device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int cap_near, int cap_items)
+__device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int cap_near, int cap_items,
+                                           bool keep = false)
 {
     PkCostSmem s;
     unsigned char* p = base;
@@ -84,6 +91,7 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
     // 8-byte arrays next: every offset up to here is a multiple of 16
     s.red = (double*)p; p += 32 * 8;
     s.redl = (long long*)p; p += 32 * 8;
+    if (keep) p += 32 * 4;   // pk_disp
     s.acc_lo = (unsigned*)p; p += (size_t)n_max * 12;
     s.acc_hi = (unsigned*)p; p += (size_t)n_max * 12;
     s.piece = (float2*)p; p += 16 * 8;
@@ -93,6 +101,7 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
     s.piece_nv = (int*)p; p += 16;
     s.count = (int*)p; p += 16;
     s.cnt = (unsigned int*)p; p += 16;
+    if (keep) p += 16;   // pk_nlist
     s.grid_cap = pk_grid_cap(n_max);
     s.cell_start = (int*)p; p += (size_t)(s.grid_cap + 1) * 4;
     s.cell_fill = (int*)p; p += (size_t)s.grid_cap * 4;
@@ -106,6 +115,12 @@ __device__ inline PkCostSmem pk_cost_carve(unsigned char* base, int n_max, int c
     s.n_cap = n_max;
     return s;
 }
+
+// Arrays placed right after cnt and redl by a carve with keep; derived from
+// them rather than held as pointers of their own (fewer live registers around
+// the clipper).
+__device__ __forceinline__ int* pk_nlist(const PkCostSmem& sm) { return (int*)(sm.cnt + 4); }
+__device__ __forceinline__ float* pk_disp(const PkCostSmem& sm) { return (float*)(sm.redl + 32); }
 
 // ---------------------------------------------------------------------------
 // Convex piece intersection area with the gradient of both rigid poses.
@@ -508,17 +523,33 @@ __device__ __forceinline__ PkQuad pk_load_quad(const PkCostSmem& sm, int p, floa
     return q;
 }
 
+// Centre-distance cull, rounded the same way wherever it is evaluated.  Swapping A and B
+// gives the same answer: rounding is symmetric under negation.
+__device__ __forceinline__ int pk_is_near(float4 A, float4 B, float cutoff)
+{
+    const float dx = __fsub_rn(B.x, A.x), dy = __fsub_rn(B.y, A.y);
+    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) <= cutoff;
+}
+
 // Phase B: evaluate every listed item; returns this thread's fixed-point
 // pair total.  Items: i (11 bits) | j (11 bits) | pi (2) | pj (2).
+// filter (LUT only): the list is a kept near list, so a pair is looked up only
+// if it passes the centre cull now; the kept pairs are counted.
 template <int MODE>
 __device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, const uint32_t* list, int count,
-                                                      float w_pair, const PkLut& lut)
+                                                      float w_pair, const PkLut& lut, bool filter = false,
+                                                      float cutoff = 0.f)
 {
     long long tot = 0;
+    unsigned kept = 0;
     for (int w = threadIdx.x; w < count; w += blockDim.x) {
         const uint32_t it = list[w];
         const int i = it & 2047, j = (it >> 11) & 2047;
         const float4 A = sm.pose[i], B = sm.pose[j];
+        if (MODE == PK_PAIR_LUT && filter) {
+            if (!pk_is_near(A, B, cutoff)) continue;
+            ++kept;
+        }
         const float2 d = make_float2(B.x - A.x, B.y - A.y);
         float val;
         float3 gi, gj;
@@ -571,14 +602,11 @@ __device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, cons
             pk_acc_add2(sm, j, make_float3(w_pair * gj.x, w_pair * gj.y, w_pair * gj.z));
         }
     }
+    if (MODE == PK_PAIR_LUT && filter) {
+        kept = __reduce_add_sync(PK_FULL_MASK, kept);
+        if ((threadIdx.x & 31) == 0 && kept) { atomicAdd(&sm.cnt[1], kept); atomicAdd(&sm.cnt[2], kept); }
+    }
     return tot;
-}
-
-// Centre-distance cull, rounded the same way wherever it is evaluated.
-__device__ __forceinline__ int pk_is_near(float4 A, float4 B, float cutoff)
-{
-    const float dx = __fsub_rn(B.x, A.x), dy = __fsub_rn(B.y, A.y);
-    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) <= cutoff;
 }
 
 // Sorted-position ranges [b0, b1) and [b2, b3) of the half neighbourhood of
@@ -601,23 +629,41 @@ __device__ __forceinline__ void pk_half_neighbourhood(const PkCostSmem& sm, int 
 
 // Processes the cn near pairs of the list: the LUT looks them up directly;
 // the analytic modes expand each into the piece pairs whose boxes overlap and
-// evaluate those in chunks.  All threads call it; it ends with a barrier.
-template <int MODE>
+// evaluate those in chunks.  Filter: the list is a kept near list (pairs
+// within a wider distance when it was built), so each pair is first tested
+// against the centre cutoff at the current poses and the pairs that pass are
+// counted; without it every listed pair is near.  All threads call it; it
+// ends with a barrier.
+// KEEP: the caller keeps near lists; the filter flag is then pk_nlist(sm)[2],
+// read where it is used (nothing extra stays live across the clipper).
+template <int MODE, bool KEEP>
 __device__ __forceinline__ long long pk_flush_near(const PkCostSmem& sm, int cn, const PkCostSpec& spec, int T)
 {
     long long tot = 0;
     const int lane = threadIdx.x & 31;
     if (MODE == PK_PAIR_LUT) {
-        if (threadIdx.x == 0) sm.cnt[2] += (unsigned)cn;
-        tot += pk_process_items<MODE>(sm, sm.near, cn, spec.w_pair, spec.lut);
+        const bool filter = KEEP && pk_nlist(sm)[2] != 0;
+        if (threadIdx.x == 0 && !filter) sm.cnt[2] += (unsigned)cn;
+        tot += pk_process_items<MODE>(sm, sm.near, cn, spec.w_pair, spec.lut, filter, c_geom.cutoff_sq);
     } else {
         for (int c0 = 0; c0 < cn; c0 += T) {
             const int w = c0 + threadIdx.x;
+            const bool filter = KEEP && pk_nlist(sm)[2] != 0;
             uint32_t mask = 0, ij = 0;
+            bool keep = false;
+            float4 A, B;
             if (w < cn) {
                 ij = sm.near[w];
+                A = sm.pose[ij & 2047];
+                B = sm.pose[(ij >> 11) & 2047];
+                keep = !filter || pk_is_near(A, B, c_geom.cutoff_sq);
+            }
+            if (filter) {
+                const unsigned kb = __ballot_sync(PK_FULL_MASK, keep);
+                if (lane == 0 && kb) atomicAdd(&sm.cnt[1], (unsigned)__popc(kb));
+            }
+            if (keep) {
                 const int i = ij & 2047, j = (ij >> 11) & 2047;
-                const float4 A = sm.pose[i], B = sm.pose[j];
                 const float dx = B.x - A.x, dy = B.y - A.y;
 #pragma unroll
                 for (int p = 0; p < 4; ++p) {
@@ -707,12 +753,193 @@ struct PkEvalOut {
     double cost;
 };
 
+// Skin of the kept near lists (below), as a fraction of the cutoff distance.
+#define PK_NEAR_SKIN 0.17f   // skin / cutoff distance
+
+__device__ __forceinline__ float pk_near_skin() { return PK_NEAR_SKIN * sqrtf(c_geom.cutoff_sq); }
+
+// Broad phase on a uniform grid of cells at least the interaction distance
+// wide: tree i only meets trees of the 3 x 3 cells around its own, and each
+// pair is found once, from its lower index.  Builds the grid (sm.cell_start,
+// sm.sorted, sm.tcell), counts each sorted position's near pairs (pass 1)
+// and scans the counts into sm.near_start; returns the grid's (gx, gy).
+// build: take pairs within cutoff + skin for a kept list, falling back to the
+// cutoff (and to no kept lists from then on) when they do not fit the near
+// list in one piece.  Leaves pk_nlist(sm)[2] (list kept) and [3] (the
+// distance pass 2 must use) for the caller, visible after its barriers.
+// KEEP: the caller keeps near lists (the flags above); without it build is
+// false and nothing is left in pk_nlist.  All threads call it.
+template <bool KEEP>
+__device__ __forceinline__ int2 pk_broad_phase(const PkCostSmem& sm, int n, bool build)
+{
+    const int T = blockDim.x;
+    const float cutoff = c_geom.cutoff_sq;
+    float cut_list = cutoff;
+    if (build) {
+        const float r = sqrtf(cutoff) + pk_near_skin();
+        cut_list = r * r;
+    }
+    int gx = 1, gy = 1;
+    float4 bb = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, -3.4e38f);   // (-min x, max x, -min y, max y)
+    for (int t = threadIdx.x; t < n; t += T) {
+        const float4 A = sm.pose[t];
+        bb.x = fmaxf(bb.x, -A.x); bb.y = fmaxf(bb.y, A.x);
+        bb.z = fmaxf(bb.z, -A.y); bb.w = fmaxf(bb.w, A.y);
+    }
+    bb = pk_block_max4(bb, (float*)sm.red);
+    const float x0 = -bb.x, y0 = -bb.z;
+    const float wx = fmaxf(bb.y - x0, 0.f), wy = fmaxf(bb.w - y0, 0.f);
+    // 1 % wider than the interaction distance, so rounding in the cell
+    // index never puts two interacting trees two cells apart
+    float cs = sqrtf(cut_list) * 1.01f;
+    for (int tries = 0; tries < 64; ++tries) {
+        gx = (int)fminf(wx / cs, 2048.f) + 1;
+        gy = (int)fminf(wy / cs, 2048.f) + 1;
+        if (gx * gy <= sm.grid_cap) break;
+        cs *= 1.25f;
+    }
+    if (gx * gy > sm.grid_cap) { gx = 1; gy = 1; cs = 3.4e38f; }   // non-finite extent: one cell
+    const float inv = 1.0f / cs;
+    const int ncell = gx * gy;
+    for (int c = threadIdx.x; c < ncell; c += T) sm.cell_fill[c] = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += T) {
+        const float4 A = sm.pose[t];
+        const int cx = min(gx - 1, max(0, (int)((A.x - x0) * inv)));
+        const int cy = min(gy - 1, max(0, (int)((A.y - y0) * inv)));
+        const int c = cy * gx + cx;
+        sm.tcell[t] = c;
+        atomicAdd(&sm.cell_fill[c], 1);
+    }
+    __syncthreads();
+    pk_block_exclusive_scan(sm.cell_fill, sm.cell_start, ncell, (int*)sm.redl);
+    for (int c = threadIdx.x; c < ncell; c += T) sm.cell_fill[c] = sm.cell_start[c];
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += T) sm.sorted[atomicAdd(&sm.cell_fill[sm.tcell[t]], 1)] = t;
+    __syncthreads();
+
+    // Half neighbourhood of sorted position a in cell (cx, cy): the rest
+    // of its own cell and the cell to its right (one contiguous range of
+    // the sorted order), and cells cx-1..cx+1 of the row above (another).
+    // Every pair of trees in touching cells is found exactly once.
+    // Pass 1 counts the near pairs of each position, a scan turns the
+    // counts into list offsets, and pass 2 writes them in chunks that fit
+    // the near list, each chunk flushed before the next is written.
+    unsigned tested = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int a = threadIdx.x; a < n; a += T) {
+            int b0, b1, b2, b3;
+            pk_half_neighbourhood(sm, a, gx, gy, b0, b1, b2, b3);
+            tested += (unsigned)(b1 - b0 + b3 - b2);
+            const float4 A = sm.pose[sm.sorted[a]];
+            int k = 0;
+            for (int b = b0; b < b1; ++b) k += pk_is_near(A, sm.pose[sm.sorted[b]], cut_list);
+            for (int b = b2; b < b3; ++b) k += pk_is_near(A, sm.pose[sm.sorted[b]], cut_list);
+            sm.near_cnt[a] = k;
+        }
+        if (KEEP && threadIdx.x == 0) {
+            // read by pass 2 and by the flush (after the scan's barriers)
+            pk_nlist(sm)[2] = build;
+            ((float*)pk_nlist(sm))[3] = cut_list;
+        }
+        __syncthreads();
+        pk_block_exclusive_scan(sm.near_cnt, sm.near_start, n, (int*)sm.redl);
+        // a kept list must fit the near list in one piece; when it does
+        // not, count again at the cutoff and keep no lists from now on
+        if (!KEEP || !build || sm.near_start[n] <= sm.cap_near) break;
+        build = false;
+        cut_list = cutoff;
+        if (threadIdx.x == 0) pk_nlist(sm)[0] = -1;
+    }
+    atomicAdd(&sm.cnt[0], tested);
+    return make_int2(gx, gy);
+}
+
+// The fused relaxation calls the broad phase and pass 2 out of line: with
+// kept lists they run once per several evaluations, and their code then stays
+// out of the hot loop's way.  A one-shot cost evaluation inlines them.  The
+// out-of-line forms take the carve's sizes, not the caller's PkCostSmem (whose
+// address would pin it to local memory), and carve the dynamic shared memory
+// again: every kernel that evaluates costs places the cost arrays at its base.
+__device__ __noinline__ int2 pk_broad_phase_outlined(int n_cap, int cap_near, int cap_items, int n, bool build)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    const PkCostSmem sm = pk_cost_carve(pk_smem, n_cap, cap_near, cap_items, true);
+    return pk_broad_phase<true>(sm, n, build);
+}
+
+// Pass 2: writes the near pairs of the longest run of sorted positions from
+// a0 whose pairs fit the near list into sm.near, and keeps the list when
+// pk_broad_phase built a kept one (the run is then every position).  Returns
+// (end of the run, pairs written).  All threads call it; the pairs are
+// written (behind a barrier) when it returns.
+template <bool KEEP>
+__device__ __forceinline__ int2 pk_write_near(const PkCostSmem& sm, int n, int a0, int gx, int gy)
+{
+    const int T = blockDim.x;
+    // the longest run of positions from a0 whose pairs fit the list
+    // (a single position's pairs always do: cap_near >= n_max)
+    int lo = a0 + 1, hi = n;
+    const int lim = sm.near_start[a0] + sm.cap_near;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sm.near_start[mid] <= lim) lo = mid; else hi = mid - 1;
+    }
+    const int a1 = lo, base = sm.near_start[a0];
+    const int cn = sm.near_start[a1] - base;
+    const float cut2 = KEEP ? ((const float*)pk_nlist(sm))[3] : c_geom.cutoff_sq;   // pass 1's distance
+    for (int a = a0 + threadIdx.x; a < a1; a += T) {
+        int b0, b1, b2, b3;
+        pk_half_neighbourhood(sm, a, gx, gy, b0, b1, b2, b3);
+        const int ia = sm.sorted[a];
+        const float4 A = sm.pose[ia];
+        uint32_t* out = sm.near + (sm.near_start[a] - base);
+        const int kmax = sm.near_cnt[a];
+        int k = 0;
+        for (int b = b0; b < b3 && k < kmax; ++b) {
+            if (b == b1) { b = b2; if (b >= b3) break; }
+            const int ib = sm.sorted[b];
+            if (pk_is_near(A, sm.pose[ib], cut2))
+                out[k++] = (uint32_t)min(ia, ib) | ((uint32_t)max(ia, ib) << 11);
+        }
+    }
+    __syncthreads();
+    if (KEEP && pk_nlist(sm)[2]) {
+        // the whole list is this one chunk: keep it, with the
+        // positions it was built at in the grid's arrays (dead from here)
+        for (int t = threadIdx.x; t < n; t += T) {
+            const float4 A = sm.pose[t];
+            ((float*)sm.sorted)[t] = A.x;
+            ((float*)sm.tcell)[t] = A.y;
+        }
+        if (threadIdx.x == 0) { pk_nlist(sm)[0] = 1; pk_nlist(sm)[1] = cn; }
+    } else if (threadIdx.x == 0) {
+        sm.cnt[1] += (unsigned)cn;
+    }
+    return make_int2(a1, cn);
+}
+
+__device__ __noinline__ int2 pk_write_near_outlined(int n_cap, int cap_near, int cap_items, int n, int a0, int gx,
+                                                   int gy)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    const PkCostSmem sm = pk_cost_carve(pk_smem, n_cap, cap_near, cap_items, true);
+    return pk_write_near<true>(sm, n, a0, gx, gy);
+}
+
 // Evaluate one instance.  X: 3n floats (global or shared), H: 3 floats or
 // NULL.  G: 3n floats or NULL (written, not accumulated); GH: 3 floats or
 // NULL.  Must be called by every thread of the block.
 // SYM: the packing may be symmetric (spec.symmetry > 1); the plain
 // instantiation keeps no symmetry state in registers.
-template <int MODE, bool SYM>
+// Kept near lists (KEEP, the fused relaxation only).  The list built by
+// one evaluation holds every pair within cutoff + skin; a later evaluation
+// reuses it, without building the cell grid, while no tree has moved by
+// more than skin / (2 sqrt 2) per coordinate since, re-applying the exact
+// centre cull to each listed pair.  Any pair near now was then within
+// cutoff + skin, so the pairs evaluated are the same as a fresh grid's, and
+// the fixed-point sums make the result independent of their order.
+template <int MODE, bool SYM, bool KEEP = false>
 __device__ double pk_eval_instance(const float* X, int ng, const float* H, const PkCostSpec& spec,
                                    float* G, float* GH, const PkCostSmem& sm)
 {
@@ -733,11 +960,20 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
         soa[8 * (threadIdx.x >> 2) + 4 + (threadIdx.x & 3)] = v.y;
     }
     if (threadIdx.x < 4) sm.piece_nv[threadIdx.x] = c_geom.piece_nv[threadIdx.x];
+    // kept list state, written by the last evaluation that built the grid
+    const int nstate = KEEP ? pk_nlist(sm)[0] : -1;
+    float disp = 0.f;   // largest coordinate change of this thread's trees since the list was built
     __syncthreads();
     // ---- phase 0: per tree -------------------------------------------------
     for (int t = threadIdx.x; t < n; t += T) {
         float x, y, th;
         pk_image_pose(X, ng, sym, t, x, y, th);
+        if (nstate == 1) {
+            // positions when the list was built, kept in the grid's dead arrays
+            const float dm = fmaxf(fabsf(__fsub_rn(x, ((const float*)sm.sorted)[t])),
+                                   fabsf(__fsub_rn(y, ((const float*)sm.tcell)[t])));
+            disp = dm <= 1e30f ? fmaxf(disp, dm) : 3.4e38f;   // NaN or infinite: rebuild
+        }
         float s, c;
         sincosf(th, &s, &c);
         sm.pose[t] = make_float4(x, y, c, s);
@@ -800,105 +1036,46 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
         *sm.count = 0;
         sm.cnt[3] += 1;
     }
+    if (nstate == 1) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) disp = fmaxf(disp, __shfl_xor_sync(PK_FULL_MASK, disp, o));
+        if ((threadIdx.x & 31) == 0) pk_disp(sm)[threadIdx.x >> 5] = disp;
+    }
     __syncthreads();
+    bool reuse = false;
+    if (nstate == 1) {
+        float dm = 0.f;
+        for (int w = 0; w < (T >> 5); ++w) dm = fmaxf(dm, pk_disp(sm)[w]);
+        // a pair's distance moved by at most 2 sqrt 2 dm; 1e-4 covers the rounding
+        reuse = 2.8285f * dm + 1e-4f < pk_near_skin();
+    }
 
     // ---- phases A + B: pairs -------------------------------------------------
     long long pair_tot = 0;
     if (MODE != PK_PAIR_NONE && n > 1) {
-        const float cutoff = c_geom.cutoff_sq;
-        // Broad phase on a uniform grid of cells at least the interaction
-        // distance wide: tree i only meets trees of the 3 x 3 cells around
-        // its own, and each pair is found once, from its lower index.
-        float4 bb = make_float4(-3.4e38f, -3.4e38f, -3.4e38f, -3.4e38f);   // (-min x, max x, -min y, max y)
-        for (int t = threadIdx.x; t < n; t += T) {
-            const float4 A = sm.pose[t];
-            bb.x = fmaxf(bb.x, -A.x); bb.y = fmaxf(bb.y, A.x);
-            bb.z = fmaxf(bb.z, -A.y); bb.w = fmaxf(bb.w, A.y);
-        }
-        bb = pk_block_max4(bb, (float*)sm.red);
-        const float x0 = -bb.x, y0 = -bb.z;
-        const float wx = fmaxf(bb.y - x0, 0.f), wy = fmaxf(bb.w - y0, 0.f);
-        // 1 % wider than the interaction distance, so rounding in the cell
-        // index never puts two interacting trees two cells apart
-        float cs = sqrtf(cutoff) * 1.01f;
         int gx = 1, gy = 1;
-        for (int tries = 0; tries < 64; ++tries) {
-            gx = (int)fminf(wx / cs, 2048.f) + 1;
-            gy = (int)fminf(wy / cs, 2048.f) + 1;
-            if (gx * gy <= sm.grid_cap) break;
-            cs *= 1.25f;
+        int a0 = reuse ? -1 : 0;   // -1: flush the kept list
+        if (!reuse) {
+            // without a kept list to reuse, build one this time (nstate >= 0)
+            const int2 g = KEEP ? pk_broad_phase_outlined(sm.n_cap, sm.cap_near, sm.cap_items, n, nstate >= 0)
+                                : pk_broad_phase<false>(sm, n, false);
+            gx = g.x;
+            gy = g.y;
         }
-        if (gx * gy > sm.grid_cap) { gx = 1; gy = 1; cs = 3.4e38f; }   // non-finite extent: one cell
-        const float inv = 1.0f / cs;
-        const int ncell = gx * gy;
-        for (int c = threadIdx.x; c < ncell; c += T) sm.cell_fill[c] = 0;
-        __syncthreads();
-        for (int t = threadIdx.x; t < n; t += T) {
-            const float4 A = sm.pose[t];
-            const int cx = min(gx - 1, max(0, (int)((A.x - x0) * inv)));
-            const int cy = min(gy - 1, max(0, (int)((A.y - y0) * inv)));
-            const int c = cy * gx + cx;
-            sm.tcell[t] = c;
-            atomicAdd(&sm.cell_fill[c], 1);
-        }
-        __syncthreads();
-        pk_block_exclusive_scan(sm.cell_fill, sm.cell_start, ncell, (int*)sm.redl);
-        for (int c = threadIdx.x; c < ncell; c += T) sm.cell_fill[c] = sm.cell_start[c];
-        __syncthreads();
-        for (int t = threadIdx.x; t < n; t += T) sm.sorted[atomicAdd(&sm.cell_fill[sm.tcell[t]], 1)] = t;
-        __syncthreads();
-
-        // Half neighbourhood of sorted position a in cell (cx, cy): the rest
-        // of its own cell and the cell to its right (one contiguous range of
-        // the sorted order), and cells cx-1..cx+1 of the row above (another).
-        // Every pair of trees in touching cells is found exactly once.
-        // Pass 1 counts the near pairs of each position, a scan turns the
-        // counts into list offsets, and pass 2 writes them in chunks that fit
-        // the near list, each chunk flushed before the next is written.
-        unsigned tested = 0;
-        for (int a = threadIdx.x; a < n; a += T) {
-            int b0, b1, b2, b3;
-            pk_half_neighbourhood(sm, a, gx, gy, b0, b1, b2, b3);
-            tested += (unsigned)(b1 - b0 + b3 - b2);
-            const float4 A = sm.pose[sm.sorted[a]];
-            int k = 0;
-            for (int b = b0; b < b1; ++b) k += pk_is_near(A, sm.pose[sm.sorted[b]], cutoff);
-            for (int b = b2; b < b3; ++b) k += pk_is_near(A, sm.pose[sm.sorted[b]], cutoff);
-            sm.near_cnt[a] = k;
-        }
-        __syncthreads();
-        pk_block_exclusive_scan(sm.near_cnt, sm.near_start, n, (int*)sm.redl);
-        atomicAdd(&sm.cnt[0], tested);
-        for (int a0 = 0; a0 < n;) {
-            // the longest run of positions from a0 whose pairs fit the list
-            // (a single position's pairs always do: cap_near >= n_max)
-            int lo = a0 + 1, hi = n;
-            const int lim = sm.near_start[a0] + sm.cap_near;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (sm.near_start[mid] <= lim) lo = mid; else hi = mid - 1;
+        while (a0 < n) {
+            int cn;
+            if (a0 < 0) {
+                // the kept list (pk_nlist(sm)[2] is still set from when it was built)
+                cn = pk_nlist(sm)[1];
+                if (threadIdx.x == 0) sm.cnt[0] += (unsigned)cn;
+                a0 = n;
+            } else {
+                const int2 r = KEEP ? pk_write_near_outlined(sm.n_cap, sm.cap_near, sm.cap_items, n, a0, gx, gy)
+                                    : pk_write_near<false>(sm, n, a0, gx, gy);
+                a0 = r.x;
+                cn = r.y;
             }
-            const int a1 = lo, base = sm.near_start[a0];
-            const int cn = sm.near_start[a1] - base;
-            for (int a = a0 + threadIdx.x; a < a1; a += T) {
-                int b0, b1, b2, b3;
-                pk_half_neighbourhood(sm, a, gx, gy, b0, b1, b2, b3);
-                const int ia = sm.sorted[a];
-                const float4 A = sm.pose[ia];
-                uint32_t* out = sm.near + (sm.near_start[a] - base);
-                const int kmax = sm.near_cnt[a];
-                int k = 0;
-                for (int b = b0; b < b3 && k < kmax; ++b) {
-                    if (b == b1) { b = b2; if (b >= b3) break; }
-                    const int ib = sm.sorted[b];
-                    if (pk_is_near(A, sm.pose[ib], cutoff))
-                        out[k++] = (uint32_t)min(ia, ib) | ((uint32_t)max(ia, ib) << 11);
-                }
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) sm.cnt[1] += (unsigned)cn;
-            if (cn > 0) pair_tot += pk_flush_near<MODE>(sm, cn, spec, T);
-            a0 = a1;
+            if (cn > 0) pair_tot += pk_flush_near<MODE, KEEP>(sm, cn, spec, T);
         }
     }
 

@@ -413,11 +413,17 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
     const int N = 3 * n + 3;
     const int m = prm.history;
     bool need_eval = !resume, final_pending = false, want_grad = true, skip_update = resume;
+    // Kept near lists when the step bound lets a list serve at least four
+    // evaluations (every coordinate moves at most max_step per step); the
+    // first evaluation of this call builds one.
+    if (threadIdx.x == 0)
+        pk_nlist(sm)[0] = (prm.has_max_step && 4.f * 2.8285f * prm.max_step + 1e-4f < pk_near_skin()) ? 0 : -1;
     for (;;) {
         if (need_eval) {
             __syncthreads();   // x complete
-            const double L = pk_eval_instance<MODE, SYM>(x, n, use_h ? x + 3 * n : nullptr, spec, want_grad ? g : nullptr,
-                                                    (want_grad && use_h) ? g + 3 * n : nullptr, sm);
+            const double L = pk_eval_instance<MODE, SYM, true>(x, n, use_h ? x + 3 * n : nullptr, spec,
+                                                          want_grad ? g : nullptr,
+                                                          (want_grad && use_h) ? g + 3 * n : nullptr, sm);
             v.loss = (float)L;
         }
         if (final_pending) return true;
@@ -542,9 +548,9 @@ __device__ void pk_relax_instance(int e, const float* __restrict__ xyt_in, const
     const int NM = 3 * n_max + 3;
     const int m = prm.history;
     const int nps = n_max * (SYM ? pk_symmetry(spec) : 1);   // phenotype trees sized in shared memory
-    PkCostSmem sm = pk_cost_carve(smem, nps, cap_near, cap_items);
+    PkCostSmem sm = pk_cost_carve(smem, nps, cap_near, cap_items, true);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
-    float* x = (float*)(smem + pk_cost_smem_bytes(nps, cap_near, cap_items));
+    float* x = (float*)(smem + pk_cost_smem_bytes(nps, cap_near, cap_items, true));
     float* g = x + NM;
     float* pg = g + NM;
     float* d = pg + NM;
@@ -630,9 +636,9 @@ __global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict
     p.max_iter = J->max_iter;
     p.max_eval = J->max_iter * 5 / 4;
     p.final_eval = 1;
-    PkCostSmem sm = pk_cost_carve(pk_smem, nps, cap_near, cap_items);
+    PkCostSmem sm = pk_cost_carve(pk_smem, nps, cap_near, cap_items, true);
     if (threadIdx.x < 4) sm.cnt[threadIdx.x] = 0;
-    float* x = (float*)(pk_smem + pk_cost_smem_bytes(nps, cap_near, cap_items));
+    float* x = (float*)(pk_smem + pk_cost_smem_bytes(nps, cap_near, cap_items, true));
     float* g = x + NM;
     float* pg = g + NM;
     float* d = pg + NM;
@@ -679,7 +685,7 @@ __global__ void __launch_bounds__(256, 3) pk_relax_jobs_kernel(PkJob* __restrict
 static size_t pk_relax_smem_bytes(int n_max, int sym, int cap_near, int cap_items, int m)
 {
     const int NM = 3 * n_max + 3;
-    return pk_cost_smem_bytes(n_max * sym, cap_near, cap_items) +
+    return pk_cost_smem_bytes(n_max * sym, cap_near, cap_items, true) +
            ((size_t)4 * NM + 2 * (size_t)m + pk_canon_red_len(NM)) * 4;
 }
 
