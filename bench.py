@@ -183,11 +183,12 @@ FLOPS_PER_HIST_ELEM = 10
 FLOPS_PER_ITER_ELEM = 16
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one relaxation
-# launch, from a one-pass ncu capture of that launch, per (E, n, iterations,
-# history); other configurations report null.  Most of it is L-BFGS history
-# (2 m (3n + 3) floats per packing) written back from L2 while packings run;
-# a finished packing's history is discarded from L2, not written back.
-TRAFFIC_BYTES = {(4096, 200, 200, 10): 61.5e6}
+# launch, from a one-pass ncu capture of that launch (the mean of two
+# launches), per (E, n, iterations, history); other configurations report
+# null.  Most of it is written back from L2 while packings run: L-BFGS history
+# (2 m (3n + 3) floats per packing; a finished packing's history is discarded
+# from L2, not written back) and spilled registers evicted with it.
+TRAFFIC_BYTES = {(4096, 200, 200, 10): 107.1e6}
 HBM_FALLBACK_GBPS = 6650.0
 
 

@@ -754,7 +754,8 @@ struct PkEvalOut {
 };
 
 // Skin of the kept near lists (below), as a fraction of the cutoff distance.
-#define PK_NEAR_SKIN 0.17f   // skin / cutoff distance
+// 0.22 relaxed 4096 x n = 200 (max_step 0.01) fastest of 0.12, 0.17, 0.22, 0.26.
+#define PK_NEAR_SKIN 0.22f   // skin / cutoff distance
 
 __device__ __forceinline__ float pk_near_skin() { return PK_NEAR_SKIN * sqrtf(c_geom.cutoff_sq); }
 
