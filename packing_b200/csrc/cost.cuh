@@ -542,7 +542,17 @@ __device__ __forceinline__ long long pk_process_items(const PkCostSmem& sm, cons
 {
     long long tot = 0;
     unsigned kept = 0;
-    for (int w = threadIdx.x; w < count; w += blockDim.x) {
+    const int nwarps = blockDim.x >> 5;
+    for (int base = 0; base < count; base += blockDim.x) {
+        // Analytic modes, full rounds: a warp's lanes take items nwarps apart.
+        // Consecutive items share trees (a near pair's piece pairs, a tree's
+        // near pairs), and spread over warps their accumulator atomics stop
+        // hitting the same addresses within a warp (1 % at 4096 x n = 200;
+        // the same bits).  The LUT's lookups keep the contiguous order.
+        const int w = MODE != PK_PAIR_LUT && base + (int)blockDim.x <= count
+                          ? base + (int)(threadIdx.x & 31) * nwarps + (int)(threadIdx.x >> 5)
+                          : base + (int)threadIdx.x;
+        if (w >= count) continue;
         const uint32_t it = list[w];
         const int i = it & 2047, j = (it >> 11) & 2047;
         const float4 A = sm.pose[i], B = sm.pose[j];
