@@ -639,13 +639,12 @@ __device__ __forceinline__ void pk_half_neighbourhood(const PkCostSmem& sm, int 
 
 // Processes the cn near pairs of the list: the LUT looks them up directly;
 // the analytic modes expand each into the piece pairs whose boxes overlap and
-// evaluate those in chunks.  Filter: the list is a kept near list (pairs
-// within a wider distance when it was built), so each pair is first tested
-// against the centre cutoff at the current poses and the pairs that pass are
-// counted; without it every listed pair is near.  All threads call it; it
-// ends with a barrier.
-// KEEP: the caller keeps near lists; the filter flag is then pk_nlist(sm)[2],
-// read where it is used (nothing extra stays live across the clipper).
+// evaluate those in chunks.  With KEEP the list may be a kept near list
+// (pk_nlist(sm)[2] set), whose pairs were within cutoff + skin when it was
+// built: each pair is then first tested against the centre cutoff at the
+// current poses, and the pairs that pass are counted.  The flag is read where
+// it is used, so nothing extra stays live across the clipper.  Otherwise every
+// listed pair is near.  All threads call it; it ends with a barrier.
 template <int MODE, bool KEEP>
 __device__ __forceinline__ long long pk_flush_near(const PkCostSmem& sm, int cn, const PkCostSpec& spec, int T)
 {
