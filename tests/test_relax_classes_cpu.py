@@ -25,8 +25,8 @@ def test_classes_cover_a_largest_first_order():
 def test_class_edge_cases():
     assert size_classes([]) == []
     assert [c.threads for c in size_classes([200, 200, 5])] == [256, 32]
-    assert [(c.n_max, c.count, c.threads) for c in size_classes([141, 140, 81, 80])] == \
-        [(141, 1, 256), (140, 2, 160), (80, 1, 96)]
+    assert [(c.n_max, c.count, c.threads) for c in size_classes([161, 160, 121, 120, 81, 80])] == \
+        [(161, 1, 256), (160, 2, 192), (120, 2, 128), (80, 1, 96)]
     with pytest.raises(ValueError):
         size_classes([5, 200])
     with pytest.raises(ValueError):
