@@ -937,6 +937,19 @@ __device__ __noinline__ int2 pk_write_near_outlined(int n_cap, int cap_near, int
     return pk_write_near<true>(sm, n, a0, gx, gy);
 }
 
+// The piece table in shared memory (SoA and AoS), from constant memory.
+__device__ __forceinline__ void pk_load_piece_table(const PkCostSmem& sm)
+{
+    if (threadIdx.x < 16) {
+        const float2 v = c_geom.piece[threadIdx.x >> 2][threadIdx.x & 3];
+        sm.piece[threadIdx.x] = v;
+        float* soa = (float*)sm.piece4;   // piece p: x at [8p + v], y at [8p + 4 + v]
+        soa[8 * (threadIdx.x >> 2) + (threadIdx.x & 3)] = v.x;
+        soa[8 * (threadIdx.x >> 2) + 4 + (threadIdx.x & 3)] = v.y;
+    }
+    if (threadIdx.x < 4) sm.piece_nv[threadIdx.x] = c_geom.piece_nv[threadIdx.x];
+}
+
 // Evaluate one instance.  X: 3n floats (global or shared), H: 3 floats or
 // NULL.  G: 3n floats or NULL (written, not accumulated); GH: 3 floats or
 // NULL.  Must be called by every thread of the block.
@@ -961,19 +974,15 @@ __device__ double pk_eval_instance(const float* X, int ng, const float* H, const
     const bool do_bnd = spec.w_boundary != 0.f && H != nullptr;
     float half = 0.f, hox = 0.f, hoy = 0.f;
     if (H) { half = H[0] * 0.5f; hox = H[1]; hoy = H[2]; }
-    // piece table into shared memory first: phase 0 reads it
-    if (threadIdx.x < 16) {
-        const float2 v = c_geom.piece[threadIdx.x >> 2][threadIdx.x & 3];
-        sm.piece[threadIdx.x] = v;
-        float* soa = (float*)sm.piece4;   // piece p: x at [8p + v], y at [8p + 4 + v]
-        soa[8 * (threadIdx.x >> 2) + (threadIdx.x & 3)] = v.x;
-        soa[8 * (threadIdx.x >> 2) + 4 + (threadIdx.x & 3)] = v.y;
+    // piece table into shared memory first: phase 0 reads it (the fused
+    // relaxation loads it once, before its first evaluation)
+    if (!KEEP) {
+        pk_load_piece_table(sm);
     }
-    if (threadIdx.x < 4) sm.piece_nv[threadIdx.x] = c_geom.piece_nv[threadIdx.x];
     // kept list state, written by the last evaluation that built the grid
     const int nstate = KEEP ? pk_nlist(sm)[0] : -1;
     float disp = 0.f;   // largest coordinate change of this thread's trees since the list was built
-    __syncthreads();
+    if (!KEEP) __syncthreads();
     // ---- phase 0: per tree -------------------------------------------------
     for (int t = threadIdx.x; t < n; t += T) {
         float x, y, th;

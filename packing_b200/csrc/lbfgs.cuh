@@ -418,6 +418,7 @@ __device__ bool pk_relax_iterate(float* x, float* g, float* pg, float* d, float*
     // first evaluation of this call builds one.
     if (threadIdx.x == 0)
         pk_nlist(sm)[0] = (prm.has_max_step && 4.f * 2.8285f * prm.max_step + 1e-4f < pk_near_skin()) ? 0 : -1;
+    pk_load_piece_table(sm);   // read after the next barrier; evaluations do not reload it
     for (;;) {
         if (need_eval) {
             __syncthreads();   // x complete
