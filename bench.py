@@ -188,7 +188,7 @@ FLOPS_PER_ITER_ELEM = 16
 # null.  Most of it is written back from L2 while packings run: L-BFGS history
 # (2 m (3n + 3) floats per packing; a finished packing's history is discarded
 # from L2, not written back) and spilled registers evicted with it.
-TRAFFIC_BYTES = {(4096, 200, 200, 10): 85.6e6}
+TRAFFIC_BYTES = {(4096, 200, 200, 10): 87.4e6}
 HBM_FALLBACK_GBPS = 6650.0
 
 
